@@ -1,0 +1,467 @@
+"""Benchmark of the batched mixed-k max_zeros path on B200 GPUs.
+
+Workload (one step): 10,000 seeded random exponent sets P of Z_7^2 with |P|
+uniform in 6..14 (distinct indices), target_distance = 1 (no early exit),
+every set's exact max_zeros -- the batched uneven evaluation configuration.
+Metric: reference-equivalent codewords/s = sum over the sets of (8^k - 1),
+the messages the reference enumerates per set, divided by the step time.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+N > 1 runs one process per GPU under torch.distributed.run; every rank
+evaluates its own seeded batch (weak scaling, no collective on the data path)
+and the step time is the maximum over ranks.  `--impl reference` times the
+reference algorithm on the host cores (the CPU restatement of kernel.py's
+batched enumeration) on a bounded sample of the same workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+N_SETS = 10_000
+K_LO, K_HI = 6, 14
+BASE_SEED = 20260
+METRIC = "GF(8) codewords/s, reference-equivalent (8^k-1 messages per code), batched mixed-k"
+UNIT = "codewords/s"
+WORKLOAD = "batched uneven evaluation: 10,000 seeded random P, |P|~U{6..14}, td=1, exact"
+POPC_PER_CODEWORD = 14.0 / 8.0  # histogram walk: 7 bins x 2 words per 8 codewords
+L2_FLUSH_BYTES = 256 << 20
+
+
+def make_workload(rank: int, n: int = N_SETS, k_lo: int = K_LO, k_hi: int = K_HI):
+    """Seeded batch of rank `rank` (rank 0 is the headline batch)."""
+    rng = np.random.default_rng(BASE_SEED + rank)
+    ks = rng.integers(k_lo, k_hi + 1, size=n)
+    return [sorted(rng.choice(49, int(k), replace=False).tolist()) for k in ks]
+
+
+def reference_messages(sets) -> float:
+    return float(sum((8 ** len(s)) - 1 for s in sets))
+
+
+def shard_bounds(n: int, rank: int, world: int) -> tuple[int, int]:
+    """Contiguous near-equal shard [lo, hi) of n items for `rank` (used when a
+    fixed batch is split across ranks)."""
+    q, r = divmod(n, world)
+    lo = rank * q + min(rank, r)
+    return lo, lo + q + (1 if rank < r else 0)
+
+
+def stratified_sample(sets, per_k: int) -> dict[int, list[list[int]]]:
+    out: dict[int, list[list[int]]] = {}
+    for s in sets:
+        lst = out.setdefault(len(s), [])
+        if len(lst) < per_k:
+            lst.append(s)
+    return out
+
+
+def k_histogram(sets) -> dict[int, int]:
+    h: dict[int, int] = {}
+    for s in sets:
+        h[len(s)] = h.get(len(s), 0) + 1
+    return h
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------
+
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+
+    def init(self, backend: str) -> None:
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+            self.pg = dist
+
+    def barrier(self) -> None:
+        if self.pg is not None:
+            self.pg.barrier()
+
+    def max(self, x: float, device=None) -> float:
+        if self.pg is None:
+            return x
+        import torch
+
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, x: float, device=None) -> float:
+        if self.pg is None:
+            return x
+        import torch
+
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self) -> None:
+        if self.pg is not None:
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu_index = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self) -> None:
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu_index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in Path(self.path).read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                rows.append(f)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        sm = [num(r[1]) for r in rows if num(r[1])]
+        smax = [num(r[2]) for r in rows if num(r[2])]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for name, val in zip(names, r[5:9]):
+                if val.lower() in ("active", "yes"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(rows),
+                "power_w_max": max((num(r[3]) or 0.0) for r in rows)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline (the reference algorithm on the host cores)
+# ---------------------------------------------------------------------------
+
+def cpu_reference_rate(sets, prefix: int, per_k: int = 2, threads: int = 0) -> dict:
+    """Reference-equivalent codewords/s of the CPU restatement of kernel.py's
+    batched enumeration on the workload's k mix, from bounded prefixes of
+    `per_k` sets per k (per-message cost grows with k, so the rate is the
+    workload-weighted harmonic mean)."""
+    from oracle import oracle as orc
+
+    M = orc.eval_matrix()
+    threads = threads or os.cpu_count() or 1
+    hist = k_histogram(sets)
+    sample = stratified_sample(sets, per_k)
+    t_msg: dict[int, float] = {}
+    total_msgs = 0
+    total_s = 0.0
+    for k, group in sorted(sample.items()):
+        t0 = time.perf_counter()
+        msgs, _ = orc.eval_prefix_batch(M, group, prefix, threads=threads)
+        dt = time.perf_counter() - t0
+        t_msg[k] = dt / max(msgs, 1)
+        total_msgs += msgs
+        total_s += dt
+    work = sum(hist[k] * ((8 ** k) - 1) for k in hist)
+    secs = sum(hist[k] * ((8 ** k) - 1) * t_msg[k] for k in hist)
+    return {"value": work / secs, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": (f"{per_k} sets per k in {K_LO}..{K_HI}, messages 1..min(8^k-1, {prefix}) "
+                       f"each ({total_msgs:.3g} messages, {total_s:.1f} s), rate weighted by the "
+                       f"10,000-set k mix"),
+            "seconds": total_s}
+
+
+def run_reference_arm(args, d: Dist) -> None:
+    if d.rank != 0:
+        return
+    sets = make_workload(0, args.n_sets, args.kmin, args.kmax)
+    prefix = 1 << 24
+    for _ in range(args.warmup):
+        cpu_reference_rate(sets, prefix)
+    vals = []
+    secs = 0.0
+    for _ in range(args.steps):
+        r = cpu_reference_rate(sets, prefix)
+        vals.append(r["value"])
+        secs += r["seconds"]
+    value = statistics.median(vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * secs / max(args.steps, 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64 (bit-sliced GF(8))",
+        "data": "synthetic (seeded)", "config": {"workload": WORKLOAD, "sample": r["sample"]},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": r["cores"], "kind": "port",
+                         "sample": r["sample"]},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# B200 arm
+# ---------------------------------------------------------------------------
+
+def measure_pipes(device: int) -> dict:
+    import ctypes
+
+    import torch
+
+    from generalized_toric_gpu_search_b200 import _lib
+
+    scratch = torch.empty(1 << 20, dtype=torch.uint8, device=f"cuda:{device}")
+    out = (ctypes.c_double * 6)()
+    _lib.check(_lib.load().tg_measure_int_pipes(device, scratch.data_ptr(), out),
+               "tg_measure_int_pipes")
+    return {"lop3_per_clk_sm": out[0], "popc_per_clk_sm": out[1], "iadd_per_clk_sm": out[2],
+            "addmax_per_clk_sm": out[3], "lop3_popc_mix_per_clk_sm": out[4],
+            "ubench_sm_mhz": out[5]}
+
+
+def run_b200_arm(args, d: Dist) -> None:
+    import torch
+
+    from generalized_toric_gpu_search_b200 import _lib
+    from generalized_toric_gpu_search_b200 import build as lib_build
+    from generalized_toric_gpu_search_b200.distance import (
+        DistanceOracleCUDABP,
+        DistanceRunner,
+        LaunchConfig,
+        ToricContext,
+        pack_sets,
+    )
+    from generalized_toric_gpu_search_b200.tables import build_eval_matrix
+
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    lib_build.build()
+    dev = d.local_rank if d.world > 1 else 0
+    torch.cuda.set_device(dev)
+    device = torch.device("cuda", dev)
+    d.init("nccl")
+    sets = make_workload(d.rank, args.n_sets, args.kmin, args.kmax)
+    M = build_eval_matrix()
+    ctx = ToricContext(dev, M)
+    cfg = LaunchConfig(tail_rows=args.tail_rows, blocks_per_sm=args.blocks_per_sm)
+    runner = DistanceRunner(ctx, cfg)
+    flat, offsets, kmax = pack_sets(sets)
+    d_idx = torch.from_numpy(flat).to(device)
+    d_off = torch.from_numpy(offsets).to(device)
+    d_out = torch.empty(len(sets), dtype=torch.int32, device=device)
+    p = runner.params(len(sets), kmax, 1)
+    ws = runner.workspace(p)
+    stream = torch.cuda.Stream(device=device)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=device)
+
+    # Two CUDA graphs: prepare (header reset, prep, scan) and the persistent walk.
+    g_prep, g_walk = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
+    with torch.cuda.stream(stream):
+        runner.run(p, d_idx, d_off, d_out, stream=stream, workspace=ws)  # warm the module
+    stream.synchronize()
+    with torch.cuda.graph(g_prep, stream=stream, capture_error_mode="thread_local"):
+        runner.prepare(p, d_idx, d_off, d_out, stream=stream, workspace=ws)
+    with torch.cuda.graph(g_walk, stream=stream, capture_error_mode="thread_local"):
+        runner.walk(p, d_out, stream=stream, workspace=ws)
+
+    def step():
+        g_prep.replay()
+        g_walk.replay()
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+    stream.synchronize()
+    check = d_out.cpu().tolist()
+    tasks, codewords, ref_msgs = runner.counters(stream)
+
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    clocks = ClockSampler(dev)
+    d.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    with torch.cuda.stream(stream):
+        for i in range(args.steps):
+            flush.zero_()  # L2 flush between steps, outside the events
+            ev[i][0].record(stream)
+            g_prep.replay()
+            ev[i][1].record(stream)
+            g_walk.replay()
+            ev[i][2].record(stream)
+    stream.synchronize()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    d.barrier()
+    step_ms = [e[0].elapsed_time(e[2]) for e in ev]
+    walk_ms = [e[1].elapsed_time(e[2]) for e in ev]
+    if d_out.cpu().tolist() != check:
+        raise SystemExit("results changed between steps")
+    total_ms = d.max(sum(step_ms), device)
+    all_ref = d.sum(ref_msgs, device)
+    value = all_ref / (total_ms / 1e3 / args.steps)
+
+    # End to end through the public API: host lists in, host list out.
+    oracle = DistanceOracleCUDABP(dev, M, cfg)
+    oracle.max_zeros_batch(sets[:64], 1)
+    h2d = flat.nbytes + offsets.nbytes
+    d2h = 4 * len(sets)
+    e2e_s = []
+    d.barrier()
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        res = oracle.max_zeros_batch(sets, 1)
+        e2e_s.append(time.perf_counter() - t0)
+    if res != check:
+        raise SystemExit("public API result differs from the device-resident run")
+    e2e_max = d.max(sum(e2e_s), device)
+    e2e_value = all_ref / (e2e_max / args.steps)
+
+    # Plain one-code-per-launch form on a stratified sample (same kernels).
+    plain = None
+    if d.rank == 0 and not args.skip_plain:
+        sample = stratified_sample(sets, 4)
+        hist = k_histogram(sets)
+        t_k = {}
+        for k, group in sample.items():
+            times = []
+            for s in group:
+                fl, of, km = pack_sets([s])
+                di, do = torch.from_numpy(fl).to(device), torch.from_numpy(of).to(device)
+                dd = torch.empty(1, dtype=torch.int32, device=device)
+                pp = runner.params(1, km, 1)
+                wws = torch.empty(max(int(1 << 20), 256), dtype=torch.uint8, device=device)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                with torch.cuda.stream(stream):
+                    e0.record(stream)
+                    runner.run(pp, di, do, dd, stream=stream, workspace=wws)
+                    e1.record(stream)
+                stream.synchronize()
+                times.append(e0.elapsed_time(e1) / 1e3)
+            t_k[k] = statistics.mean(times)
+        plain_s = sum(hist[k] * t_k[k] for k in hist)
+        plain = {"value": ref_msgs / plain_s, "unit": UNIT, "codes_per_s": len(sets) / plain_s,
+                 "sample": "4 sets per k, one launch per set, per-k mean time x k histogram"}
+
+    # Roofline of the dominant kernel (the persistent histogram walk).
+    pipes = measure_pipes(dev) if d.rank == 0 else {}
+    walk_s = statistics.mean(walk_ms) / 1e3
+    sm_count = ctx.sm_count
+    mhz = clk.get("sm_mhz") or pipes.get("ubench_sm_mhz")
+    achieved = POPC_PER_CODEWORD * codewords / walk_s
+    peak = pipes.get("popc_per_clk_sm", 16.0) * sm_count * (mhz or 1965.0) * 1e6
+
+    cpu = None
+    if d.rank == 0 and d.world == 1 and not args.skip_cpu:
+        cpu = cpu_reference_rate(sets, 1 << 26, per_k=4)
+
+    if d.rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": d.world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32 bit-sliced GF(8) (integer LOP3/POPC)",
+            "data": "synthetic (seeded random exponent sets)",
+            "config": {"workload": WORKLOAD, "n_sets_per_gpu": len(sets),
+                       "k_range": [K_LO, K_HI], "target_distance": 1,
+                       "enumeration": "orbit (projective + torus normalisation)",
+                       "variant": "histogram", "tail_rows": args.tail_rows or 4,
+                       "launch": "CUDA graphs: prepare + one persistent walk",
+                       "l2": "256 MiB write between timed steps",
+                       "parallelism": f"weak, {d.world} rank(s), no data-path collective"},
+            "codes_per_s": d.world * len(sets) / (total_ms / 1e3 / args.steps),
+            "evaluated_codewords_per_s": d.world * codewords / (total_ms / 1e3 / args.steps),
+            "evaluated_codewords_per_step": codewords, "tasks_per_step": tasks,
+            "walk_ms": statistics.mean(walk_ms),
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * e2e_max / args.steps,
+                    "api": "DistanceOracleCUDABP.max_zeros_batch(list of lists, 1)"},
+            "gpu_launches": 3 * args.steps,
+            "roofline": {"bound": "int (POPC pipe)", "achieved": achieved / 1e12,
+                         "peak": peak / 1e12, "unit": "Tpopc/s", "frac": achieved / peak,
+                         "traffic": None,
+                         "note": "1.75 POPC per codeword (14 per 8-codeword histogram); peak = "
+                                 "measured POPC/clk/SM x SMs x median SM MHz in the timed region"},
+            "int_pipes": pipes,
+            "clocks": clk,
+            "plain_form": plain,
+            "batched_vs_plain": (value / plain["value"]) if plain else None,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    del g_prep, g_walk
+    d.close()
+
+
+def main(argv=None) -> None:
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--tail-rows", type=int, default=0)
+    ap.add_argument("--blocks-per-sm", type=int, default=0)
+    ap.add_argument("--skip-plain", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--n-sets", type=int, default=N_SETS, help="sets per GPU (small cases)")
+    ap.add_argument("--kmin", type=int, default=K_LO)
+    ap.add_argument("--kmax", type=int, default=K_HI)
+    args = ap.parse_args(argv)
+    d = Dist()
+    if args.impl == "reference":
+        run_reference_arm(args, d)
+        return
+    run_b200_arm(args, d)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,72 @@
+"""Builds libtoric_b200.so (the sm_100a CUDA library) in-tree with nvcc.
+
+Usage: python -m generalized_toric_gpu_search_b200.build [--ptxas-verbose]
+"""
+
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG_DIR = Path(__file__).resolve().parent
+CSRC = PKG_DIR / "csrc"
+LIB_NAME = "libtoric_b200.so"
+LIB_PATH = PKG_DIR / LIB_NAME
+SOURCES = ["abi.cu", "distance.cu", "canonical.cu", "intpeak.cu"]
+ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def nvcc_path() -> str:
+    cand = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not Path(cand).exists():
+        raise RuntimeError("nvcc not found; the CUDA toolkit is required to build libtoric_b200")
+    return cand
+
+
+def _newest_source_mtime() -> float:
+    files = [CSRC / s for s in SOURCES] + list(CSRC.glob("*.cuh"))
+    files.append(PKG_DIR.parent / "include" / "toric_b200.h")
+    return max(f.stat().st_mtime for f in files if f.exists())
+
+
+def needs_build() -> bool:
+    return not LIB_PATH.exists() or LIB_PATH.stat().st_mtime < _newest_source_mtime()
+
+
+def build(force: bool = False, ptxas_verbose: bool = False) -> Path:
+    """Compiles the CUDA sources into LIB_PATH (skipped when up to date)."""
+    if not force and not ptxas_verbose and not needs_build():
+        return LIB_PATH
+    cmd = [
+        nvcc_path(),
+        *ARCH_FLAGS,
+        "-O3",
+        "-lineinfo",
+        "-std=c++17",
+        "--expt-relaxed-constexpr",
+        "-Xcompiler",
+        "-fPIC,-O2",
+        "-shared",
+        "-o",
+        str(LIB_PATH) + ".tmp",
+        *[str(CSRC / s) for s in SOURCES],
+    ]
+    if ptxas_verbose:
+        cmd.insert(1, "-Xptxas=-v")
+    proc = subprocess.run(cmd, cwd=str(PKG_DIR), capture_output=True, text=True)
+    if proc.returncode != 0:
+        raise RuntimeError(
+            "nvcc failed (exit %d):\n%s\n%s" % (proc.returncode, " ".join(cmd), proc.stderr)
+        )
+    if ptxas_verbose:
+        sys.stderr.write(proc.stderr)
+    os.replace(str(LIB_PATH) + ".tmp", LIB_PATH)
+    return LIB_PATH
+
+
+if __name__ == "__main__":
+    build(force=True, ptxas_verbose="--ptxas-verbose" in sys.argv)
+    print(LIB_PATH)

@@ -1,0 +1,451 @@
+// extern "C" boundary of libtoric_b200.so (declared in include/toric_b200.h):
+// argument checks, device selection, context tables and launch dispatch.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "canonical.cuh"
+#include "distance.cuh"
+
+struct tg_context {
+  int device;
+  int sm_count;
+  int is_toric;
+  uint8_t* d_M;    // 49 x 49
+  uint8_t* d_gl2;  // 2016 x 49
+};
+
+namespace tg {
+
+static thread_local char g_err[512] = "";
+
+void set_last_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  set_last_error("%s: %s (%s)", what, cudaGetErrorName(e), cudaGetErrorString(e));
+  return TG_ERR_CUDA;
+}
+
+static int invalid(const char* msg) {
+  set_last_error("%s", msg);
+  return TG_ERR_INVALID_ARGUMENT;
+}
+
+// Restores the calling thread's current device on scope exit.
+class DeviceGuard {
+ public:
+  explicit DeviceGuard(int dev) {
+    ok_ = cudaGetDevice(&prev_) == cudaSuccess;
+    err_ = cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    if (ok_) cudaSetDevice(prev_);
+  }
+  cudaError_t error() const { return err_; }
+
+ private:
+  int prev_ = 0;
+  bool ok_ = false;
+  cudaError_t err_ = cudaSuccess;
+};
+
+// The toric evaluation matrix of precompute.py:32-43: row a*7+b is x^a y^b,
+// column j is the torus point (x, y) = (1 + j/7, 1 + j%7).
+static void toric_matrix(uint8_t out[kN * kN]) {
+  auto pw = [](uint8_t base, int e) {
+    uint8_t r = 1;
+    for (int i = 0; i < e; ++i) r = gf8_mul_c(r, base);
+    return r;
+  };
+  for (int i = 0; i < kN; ++i)
+    for (int j = 0; j < kN; ++j)
+      out[i * kN + j] = gf8_mul_c(pw(uint8_t(1 + j / 7), i / 7), pw(uint8_t(1 + j % 7), i % 7));
+}
+
+// GL2(F7) as permutations of the 49 points, matrices (a b; c d) in the
+// lexicographic order of (a, b, c, d) with nonzero determinant; point (x, y)
+// maps to (a x + b y, c x + d y) (champion_search_canonical.py:61-74).
+static void gl2_table(uint8_t out[kGl2Order * kN]) {
+  int m = 0;
+  for (int a = 0; a < 7; ++a)
+    for (int b = 0; b < 7; ++b)
+      for (int c = 0; c < 7; ++c)
+        for (int d = 0; d < 7; ++d) {
+          if (((a * d - b * c) % 7 + 7) % 7 == 0) continue;
+          for (int p = 0; p < kN; ++p) {
+            const int x = p / 7, y = p % 7;
+            out[m * kN + p] = uint8_t(((a * x + b * y) % 7) * 7 + (c * x + d * y) % 7);
+          }
+          ++m;
+        }
+}
+
+}  // namespace tg
+
+using namespace tg;
+
+extern "C" {
+
+const char* tg_status_string(int status) {
+  switch (status) {
+    case TG_OK: return "TG_OK";
+    case TG_ERR_INVALID_ARGUMENT: return "TG_ERR_INVALID_ARGUMENT";
+    case TG_ERR_CUDA: return "TG_ERR_CUDA";
+    case TG_ERR_WORKSPACE: return "TG_ERR_WORKSPACE";
+    case TG_ERR_NO_DEVICE: return "TG_ERR_NO_DEVICE";
+    case TG_ERR_CAPACITY: return "TG_ERR_CAPACITY";
+    case TG_ERR_TIMEOUT: return "TG_ERR_TIMEOUT";
+    case TG_ERR_BAD_INPUT: return "TG_ERR_BAD_INPUT";
+    case TG_ERR_STATE: return "TG_ERR_STATE";
+    default: return "TG_ERR_UNKNOWN";
+  }
+}
+
+const char* tg_last_error(void) { return g_err; }
+
+int tg_abi_version(void) { return TG_ABI_VERSION; }
+
+int tg_device_count(int32_t* h_count) {
+  if (!h_count) return invalid("tg_device_count: NULL output");
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess) {
+    *h_count = 0;
+    cudaGetLastError();
+    set_last_error("cudaGetDeviceCount: %s", cudaGetErrorString(e));
+    return e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver ? TG_OK : TG_ERR_CUDA;
+  }
+  *h_count = n;
+  return TG_OK;
+}
+
+int tg_device_info(int device, int32_t* h_sm_count, int32_t* h_cc_major, int32_t* h_cc_minor,
+                   char* h_name, int32_t name_len) {
+  cudaDeviceProp prop;
+  cudaError_t e = cudaGetDeviceProperties(&prop, device);
+  if (e != cudaSuccess) {
+    set_last_error("cudaGetDeviceProperties(%d): %s", device, cudaGetErrorString(e));
+    return TG_ERR_NO_DEVICE;
+  }
+  if (h_sm_count) *h_sm_count = prop.multiProcessorCount;
+  if (h_cc_major) *h_cc_major = prop.major;
+  if (h_cc_minor) *h_cc_minor = prop.minor;
+  if (h_name && name_len > 0) {
+    std::strncpy(h_name, prop.name, size_t(name_len) - 1);
+    h_name[name_len - 1] = '\0';
+  }
+  return TG_OK;
+}
+
+int tg_context_create(int device, const int32_t* h_M, tg_context** out_ctx) {
+  if (!out_ctx) return invalid("tg_context_create: NULL out_ctx");
+  *out_ctx = nullptr;
+  if (!h_M) return invalid("tg_context_create: NULL matrix");
+  uint8_t M[kN * kN];
+  for (int i = 0; i < kN * kN; ++i) {
+    if (h_M[i] < 0 || h_M[i] > 7) return invalid("tg_context_create: matrix entries must be 0..7");
+    M[i] = uint8_t(h_M[i]);
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    set_last_error("No CUDA GPU found.");
+    return TG_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= ndev) {
+    set_last_error("device %d out of range (%d devices)", device, ndev);
+    return TG_ERR_NO_DEVICE;
+  }
+  DeviceGuard g(device);
+  if (g.error() != cudaSuccess) return cuda_fail(g.error(), "cudaSetDevice");
+  int st = upload_field_tables(device);
+  if (st) return st;
+  cudaDeviceProp prop;
+  cudaError_t e = cudaGetDeviceProperties(&prop, device);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDeviceProperties");
+  uint8_t T[kN * kN];
+  toric_matrix(T);
+  std::vector<uint8_t> gl2(size_t(kGl2Order) * kN);
+  gl2_table(gl2.data());
+  tg_context* ctx = new tg_context();
+  ctx->device = device;
+  ctx->sm_count = prop.multiProcessorCount;
+  ctx->is_toric = std::memcmp(T, M, sizeof(M)) == 0 ? 1 : 0;
+  e = cudaMalloc(&ctx->d_M, sizeof(M));
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_gl2, gl2.size());
+  if (e == cudaSuccess) e = cudaMemcpy(ctx->d_M, M, sizeof(M), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(ctx->d_gl2, gl2.data(), gl2.size(), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    if (ctx->d_M) cudaFree(ctx->d_M);
+    if (ctx->d_gl2) cudaFree(ctx->d_gl2);
+    delete ctx;
+    return cuda_fail(e, "context tables");
+  }
+  *out_ctx = ctx;
+  return TG_OK;
+}
+
+int tg_context_destroy(tg_context* ctx) {
+  if (!ctx) return TG_OK;
+  DeviceGuard g(ctx->device);
+  if (ctx->d_M) cudaFree(ctx->d_M);
+  if (ctx->d_gl2) cudaFree(ctx->d_gl2);
+  delete ctx;
+  return TG_OK;
+}
+
+int tg_context_is_toric(const tg_context* ctx, int32_t* h_is_toric) {
+  if (!ctx || !h_is_toric) return invalid("tg_context_is_toric: NULL argument");
+  *h_is_toric = ctx->is_toric;
+  return TG_OK;
+}
+
+static int check_distance_params(const tg_distance_params* p) {
+  if (!p) return invalid("NULL tg_distance_params");
+  if (p->n_sets < 0) return invalid("n_sets must be >= 0");
+  if (p->sample_count < 0) return invalid("sample_count must be >= 0");
+  if (p->sample_count > 0) {
+    if (p->k_max < 0 || p->k_max > kMaxSampledK)
+      return invalid("CUDA-BP bit-parallel kernel supports k <= 49");
+  } else if (p->k_max < 0 || p->k_max > kMaxExactK) {
+    return invalid("Exact CUDA-BP batch evaluation supports k <= 21");
+  }
+  if (p->tail_rows != 0 && (p->tail_rows < 2 || p->tail_rows > 7))
+    return invalid("tail_rows must be 0 or 2..7");
+  if (p->enumeration < TG_ENUM_AUTO || p->enumeration > TG_ENUM_ORBIT)
+    return invalid("unknown enumeration");
+  if (p->variant < TG_VARIANT_AUTO || p->variant > TG_VARIANT_DIRECT)
+    return invalid("unknown variant");
+  if (p->blocks_per_sm < 0 || p->blocks_per_sm > 16) return invalid("blocks_per_sm must be 0..16");
+  if (p->threads_per_block != 0 && p->threads_per_block != 64 && p->threads_per_block != 128 &&
+      p->threads_per_block != 256)
+    return invalid("threads_per_block must be 0, 64, 128 or 256");
+  return TG_OK;
+}
+
+int tg_distance_workspace_size(const tg_distance_params* p, size_t* h_bytes) {
+  int st = check_distance_params(p);
+  if (st) return st;
+  if (!h_bytes) return invalid("NULL h_bytes");
+  *h_bytes = ws_layout(*p).total;
+  return TG_OK;
+}
+
+static void bind_workspace(DistArgs& a, const WsLayout& L, void* ws) {
+  uint8_t* b = static_cast<uint8_t*>(ws);
+  a.hdr = reinterpret_cast<WsHeader*>(b + L.hdr);
+  a.desc = reinterpret_cast<CodeDesc*>(b + L.desc);
+  a.task_off = reinterpret_cast<uint64_t*>(b + L.task_off);
+  a.abort = reinterpret_cast<int32_t*>(b + L.abort);
+  a.basis = reinterpret_cast<V6*>(b + L.basis);
+  a.pat_cum = reinterpret_cast<uint64_t*>(b + L.pat_cum);
+  a.pat_info = reinterpret_cast<uint32_t*>(b + L.pat_info);
+  a.bitpat = reinterpret_cast<V6*>(b + L.bitpat);
+  a.basis_stride = L.basis_stride;
+  a.pat_stride = L.pat_stride;
+  a.bitpat_stride = L.bitpat_stride;
+}
+
+// Validates a max_zeros call and fills the kernel arguments.
+static int bind_distance(tg_context* ctx, const tg_distance_params* p, const int32_t* d_indices,
+                         const int64_t* d_offsets, const int32_t* d_target,
+                         const int32_t* d_set_ids, int32_t* d_out, void* d_workspace,
+                         size_t workspace_bytes, bool need_inputs, DistArgs& a) {
+  if (!ctx) return invalid("tg_max_zeros: NULL context");
+  int st = check_distance_params(p);
+  if (st) return st;
+  if (p->n_sets == 0) return TG_OK;
+  if ((need_inputs && (!d_indices || !d_offsets)) || !d_out)
+    return invalid("tg_max_zeros: NULL device pointer");
+  if (!d_workspace || (reinterpret_cast<uintptr_t>(d_workspace) & 255u))
+    return invalid("tg_max_zeros: workspace must be non-NULL and 256-byte aligned");
+  const WsLayout L = ws_layout(*p);
+  if (workspace_bytes < L.total) {
+    set_last_error("tg_max_zeros: workspace has %zu bytes, needs %zu", workspace_bytes, L.total);
+    return TG_ERR_WORKSPACE;
+  }
+  int enumeration = p->enumeration;
+  if (enumeration == TG_ENUM_AUTO) enumeration = ctx->is_toric ? TG_ENUM_ORBIT : TG_ENUM_PROJECTIVE;
+  if (enumeration == TG_ENUM_ORBIT && !ctx->is_toric)
+    return invalid("orbit enumeration needs the toric evaluation matrix");
+  int variant = p->variant;
+  if (variant == TG_VARIANT_AUTO) variant = ctx->is_toric ? TG_VARIANT_HISTOGRAM : TG_VARIANT_DIRECT;
+  if (variant == TG_VARIANT_HISTOGRAM && !ctx->is_toric)
+    return invalid("histogram variant needs the toric evaluation matrix");
+  a = DistArgs{};
+  a.idx = d_indices;
+  a.off = d_offsets;
+  a.target = d_target;
+  a.set_ids = d_set_ids;
+  a.out = d_out;
+  a.n = p->n_sets;
+  a.k_max = p->k_max;
+  a.R = default_tail_rows(*p);
+  a.enumeration = enumeration;
+  a.variant = variant;
+  a.td_default = p->target_distance;
+  a.sample_count = p->sample_count;
+  a.seed = p->sample_seed;
+  a.tab.M = ctx->d_M;
+  a.tab.gl2 = ctx->d_gl2;
+  bind_workspace(a, L, d_workspace);
+  return TG_OK;
+}
+
+static int launch_shape(const tg_distance_params* p, int* bps, int* tpb) {
+  *bps = p->blocks_per_sm > 0 ? p->blocks_per_sm : 8;
+  *tpb = p->threads_per_block > 0 ? p->threads_per_block : 128;
+  return TG_OK;
+}
+
+int tg_max_zeros_prepare(tg_context* ctx, const tg_distance_params* p, const int32_t* d_indices,
+                         const int64_t* d_offsets, const int32_t* d_target,
+                         const int32_t* d_set_ids, int32_t* d_out, void* d_workspace,
+                         size_t workspace_bytes, void* stream) {
+  DistArgs a;
+  int st = bind_distance(ctx, p, d_indices, d_offsets, d_target, d_set_ids, d_out, d_workspace,
+                         workspace_bytes, true, a);
+  if (st || p->n_sets == 0) return st;
+  DeviceGuard g(ctx->device);
+  if (g.error() != cudaSuccess) return cuda_fail(g.error(), "cudaSetDevice");
+  return run_prepare(a, static_cast<cudaStream_t>(stream));
+}
+
+int tg_max_zeros_walk(tg_context* ctx, const tg_distance_params* p, int32_t* d_out,
+                      void* d_workspace, size_t workspace_bytes, void* stream) {
+  DistArgs a;
+  int st = bind_distance(ctx, p, nullptr, nullptr, nullptr, nullptr, d_out, d_workspace,
+                         workspace_bytes, false, a);
+  if (st || p->n_sets == 0) return st;
+  DeviceGuard g(ctx->device);
+  if (g.error() != cudaSuccess) return cuda_fail(g.error(), "cudaSetDevice");
+  int bps, tpb;
+  launch_shape(p, &bps, &tpb);
+  return run_walk(a, ctx->sm_count, bps, tpb, static_cast<cudaStream_t>(stream));
+}
+
+int tg_max_zeros(tg_context* ctx, const tg_distance_params* p, const int32_t* d_indices,
+                 const int64_t* d_offsets, const int32_t* d_target, const int32_t* d_set_ids,
+                 int32_t* d_out, void* d_workspace, size_t workspace_bytes, void* stream) {
+  DistArgs a;
+  int st = bind_distance(ctx, p, d_indices, d_offsets, d_target, d_set_ids, d_out, d_workspace,
+                         workspace_bytes, true, a);
+  if (st || p->n_sets == 0) return st;
+  DeviceGuard g(ctx->device);
+  if (g.error() != cudaSuccess) return cuda_fail(g.error(), "cudaSetDevice");
+  const cudaStream_t s = static_cast<cudaStream_t>(stream);
+  st = run_prepare(a, s);
+  if (st) return st;
+  int bps, tpb;
+  launch_shape(p, &bps, &tpb);
+  return run_walk(a, ctx->sm_count, bps, tpb, s);
+}
+
+int tg_distance_status(const tg_distance_params* p, const void* d_workspace, void* stream,
+                       int32_t* h_status) {
+  int st = check_distance_params(p);
+  if (st) return st;
+  if (!d_workspace || !h_status) return invalid("tg_distance_status: NULL argument");
+  const WsLayout L = ws_layout(*p);
+  WsHeader h{};
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaMemcpyAsync(&h, static_cast<const uint8_t*>(d_workspace) + L.hdr, sizeof(h),
+                                  cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(e, "tg_distance_status");
+  *h_status = h.status;
+  return TG_OK;
+}
+
+int tg_distance_counters(const tg_distance_params* p, const void* d_workspace, void* stream,
+                         uint64_t* h_tasks, uint64_t* h_codewords, double* h_reference_messages) {
+  int st = check_distance_params(p);
+  if (st) return st;
+  if (!d_workspace) return invalid("tg_distance_counters: NULL workspace");
+  const WsLayout L = ws_layout(*p);
+  WsHeader h{};
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaMemcpyAsync(&h, static_cast<const uint8_t*>(d_workspace) + L.hdr, sizeof(h),
+                                  cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(e, "tg_distance_counters");
+  if (h_tasks) *h_tasks = h.total_tasks;
+  if (h_codewords) *h_codewords = h.codewords;
+  if (h_reference_messages) *h_reference_messages = h.ref_messages;
+  return TG_OK;
+}
+
+int tg_canonical_sets(tg_context* ctx, const int32_t* d_sets, int32_t n, int32_t k,
+                      uint64_t* d_out_mask, uint64_t* d_out_key_lo, uint64_t* d_out_key_hi,
+                      int32_t* d_status, void* stream) {
+  if (!ctx) return invalid("tg_canonical_sets: NULL context");
+  if (n < 0) return invalid("tg_canonical_sets: n must be >= 0");
+  if (k < 0 || k > kN) return invalid("tg_canonical_sets: k must be 0..49");
+  if (n == 0) return TG_OK;
+  if ((k > 0 && !d_sets) || !d_out_mask) return invalid("tg_canonical_sets: NULL device pointer");
+  DeviceGuard g(ctx->device);
+  if (g.error() != cudaSuccess) return cuda_fail(g.error(), "cudaSetDevice");
+  static const int32_t kDummy = 0;
+  return run_canonical(ctx->device, ctx->sm_count, ctx->d_gl2, k > 0 ? d_sets : &kDummy, nullptr,
+                       n, k, d_out_mask, d_out_key_lo, d_out_key_hi, d_status,
+                       static_cast<cudaStream_t>(stream));
+}
+
+int tg_canonical_masks(tg_context* ctx, const uint64_t* d_masks, int32_t n, uint64_t* d_out_mask,
+                       uint64_t* d_out_key_lo, uint64_t* d_out_key_hi, void* stream) {
+  if (!ctx) return invalid("tg_canonical_masks: NULL context");
+  if (n < 0) return invalid("tg_canonical_masks: n must be >= 0");
+  if (n == 0) return TG_OK;
+  if (!d_masks || !d_out_mask) return invalid("tg_canonical_masks: NULL device pointer");
+  DeviceGuard g(ctx->device);
+  if (g.error() != cudaSuccess) return cuda_fail(g.error(), "cudaSetDevice");
+  return run_canonical(ctx->device, ctx->sm_count, ctx->d_gl2, nullptr, d_masks, n, 0, d_out_mask,
+                       d_out_key_lo, d_out_key_hi, nullptr, static_cast<cudaStream_t>(stream));
+}
+
+int tg_hashset_bytes(int64_t capacity, size_t* h_bytes) {
+  if (!h_bytes) return invalid("tg_hashset_bytes: NULL output");
+  if (capacity < 64 || (capacity & (capacity - 1)))
+    return invalid("hash set capacity must be a power of two >= 64");
+  *h_bytes = hashset_bytes(capacity);
+  return TG_OK;
+}
+
+int tg_hashset_clear(void* d_table, int64_t capacity, void* stream) {
+  if (!d_table) return invalid("tg_hashset_clear: NULL table");
+  if (capacity < 64 || (capacity & (capacity - 1)))
+    return invalid("hash set capacity must be a power of two >= 64");
+  return run_hash_clear(d_table, capacity, static_cast<cudaStream_t>(stream));
+}
+
+int tg_hashset_insert(void* d_table, int64_t capacity, const uint64_t* d_keys, int32_t n,
+                      uint32_t call_id, uint8_t* d_is_new, int32_t* d_n_new, int32_t* d_status,
+                      void* stream) {
+  if (!d_table) return invalid("tg_hashset_insert: NULL table");
+  if (capacity < 64 || (capacity & (capacity - 1)))
+    return invalid("hash set capacity must be a power of two >= 64");
+  if (n < 0) return invalid("tg_hashset_insert: n must be >= 0");
+  if (n > 0 && !d_keys) return invalid("tg_hashset_insert: NULL keys");
+  if (call_id == 0) return invalid("tg_hashset_insert: call_id must be >= 1");
+  return run_hash_insert(d_table, capacity, d_keys, n, call_id, d_is_new, d_n_new, d_status,
+                         static_cast<cudaStream_t>(stream));
+}
+
+int tg_measure_int_pipes(int device, void* d_scratch, double* h_out6) {
+  if (!d_scratch || !h_out6) return invalid("tg_measure_int_pipes: NULL argument");
+  int32_t sm = 0;
+  int st = tg_device_info(device, &sm, nullptr, nullptr, nullptr, 0);
+  if (st) return st;
+  DeviceGuard g(device);
+  if (g.error() != cudaSuccess) return cuda_fail(g.error(), "cudaSetDevice");
+  return measure_int_pipes(sm, d_scratch, h_out6);
+}
+
+}  // extern "C"

@@ -1,0 +1,125 @@
+// Shared definitions of libtoric_b200: GF(8) arithmetic, bit-sliced codeword
+// vectors, status words and small device helpers.
+//
+// Field: GF(8) = GF(2)[x]/(x^3 + x + 1), elements 0..7 as polynomial bit
+// patterns, the modulus of gf8.py:9 (POLY = 0b1011).  A codeword of length 49
+// is stored bit-sliced: plane p holds bit p of the 49 GF(8) coordinates, the
+// coordinates 0..31 in a `lo` word and 32..48 in bits 0..16 of a `hi` word.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/toric_b200.h"
+
+namespace tg {
+
+constexpr int kN = 49;                       // code length = torus points
+constexpr int kMaxExactK = 21;               // exact enumeration limit (kernel_cuda_bp.py:270)
+constexpr int kMaxSampledK = 49;             // sampled limit (kernel_cuda_bp.py:301)
+constexpr uint32_t kHiMask = (1u << 17) - 1; // coordinates 32..48
+constexpr uint64_t kMask49 = (1ull << 49) - 1;
+constexpr int kGl2Order = 2016;              // |GL2(F7)|
+
+// Carry-less product modulo x^3 + x + 1 (gf8.py:11-21).
+constexpr uint8_t gf8_mul_c(uint8_t a, uint8_t b) {
+  uint8_t r = 0;
+  for (int i = 0; i < 3; ++i) {
+    if (b & 1) r ^= a;
+    a = static_cast<uint8_t>(a << 1);
+    if (a & 8) a ^= 0xB;
+    b >>= 1;
+  }
+  return r;
+}
+
+// Bit-sliced codeword: three planes x (lo, hi).  32 bytes with padding so a
+// vector loads as two 16-byte words.
+struct alignas(16) V6 {
+  uint32_t l0, l1, l2, h0, h1, h2, pad0, pad1;
+};
+
+__host__ __device__ __forceinline__ void v6_zero(V6& v) {
+  v.l0 = v.l1 = v.l2 = v.h0 = v.h1 = v.h2 = 0u;
+  v.pad0 = v.pad1 = 0u;
+}
+
+__device__ __forceinline__ void v6_xor(V6& a, const V6& b) {
+  a.l0 ^= b.l0; a.l1 ^= b.l1; a.l2 ^= b.l2;
+  a.h0 ^= b.h0; a.h1 ^= b.h1; a.h2 ^= b.h2;
+}
+
+// Loads a bit-sliced vector through the read-only path (two 16-byte loads).
+__device__ __forceinline__ V6 v6_ldg(const V6* p) {
+  const uint4* q = reinterpret_cast<const uint4*>(p);
+  const uint4 a = __ldg(q);
+  const uint4 b = __ldg(q + 1);
+  V6 v;
+  v.l0 = a.x; v.l1 = a.y; v.l2 = a.z; v.h0 = a.w;
+  v.h1 = b.x; v.h2 = b.y; v.pad0 = 0u; v.pad1 = 0u;
+  return v;
+}
+
+__device__ __forceinline__ void v6_stg(V6* p, const V6& v) {
+  uint4* q = reinterpret_cast<uint4*>(p);
+  q[0] = make_uint4(v.l0, v.l1, v.l2, v.h0);
+  q[1] = make_uint4(v.h1, v.h2, 0u, 0u);
+}
+
+// 3-input logic op with an immediate truth table (one LOP3).
+template <int kLut>
+__device__ __forceinline__ uint32_t lop3(uint32_t a, uint32_t b, uint32_t c) {
+  uint32_t d;
+  asm("lop3.b32 %0, %1, %2, %3, %4;" : "=r"(d) : "r"(a), "r"(b), "r"(c), "n"(kLut));
+  return d;
+}
+
+// Truth table of "(a, b, c) == (bit0, bit1, bit2) of v" for lop3 inputs
+// a = 0xF0, b = 0xCC, c = 0xAA.
+constexpr int sel_lut(int v) {
+  return ((v & 1) ? 0xF0 : 0x0F) & ((v & 2) ? 0xCC : 0x33) & ((v & 4) ? 0xAA : 0x55);
+}
+
+// Relaxed device-scope load of a flag written by other CTAs.
+__device__ __forceinline__ int ld_flag(const int32_t* p) {
+  return *reinterpret_cast<const volatile int32_t*>(p);
+}
+
+// Index of the last element of sorted a[0..n) that is <= x (a[0] <= x).
+__device__ __forceinline__ int last_le(const uint64_t* a, int n, uint64_t x) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(a + mid) <= x) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// splitmix64 finaliser (kernel_cuda_bp.py:47-52, kernel.py:10-15).
+__host__ __device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+
+// x mod (2^m - 1) for 1 <= m <= 63, by folding m-bit digits (2^m == 1).
+__host__ __device__ __forceinline__ uint64_t mod_mersenne(uint64_t x, int m) {
+  const uint64_t M = (1ull << m) - 1ull;
+  while (x > M) x = (x & M) + (x >> m);
+  return x == M ? 0ull : x;
+}
+
+// Context tables shared by the kernels (device memory of one context).
+struct DeviceTables {
+  const uint8_t* M;       // 49 x 49 matrix entries (row-major)
+  const uint8_t* gl2;     // 2016 x 49 point permutations of GL2(F7)
+};
+
+}  // namespace tg
+
+// Host-side helpers implemented in abi.cu.
+namespace tg {
+void set_last_error(const char* fmt, ...);
+int cuda_fail(cudaError_t e, const char* what);
+}  // namespace tg

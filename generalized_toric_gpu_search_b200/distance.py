@@ -1,0 +1,279 @@
+"""max_zeros oracles on the B200.
+
+`DistanceOracleCUDABP` keeps the reference interface of
+kernel_cuda_bp.py:246-323 (`device_id`, `max_zeros`, `max_zeros_batch` with
+`sample_count` / `sample_seed`) and `init_cuda_oracles_bp` (:330-347), so the
+search drivers (champion_search_canonical.py:611-647, evolve_search.py:190-220)
+use it unchanged.  All arithmetic runs in libtoric_b200.so; torch only provides
+device buffers and streams.
+
+Result contract (the reference's, kernel_cuda_bp.py:227-235): a set passes when
+max_zeros <= 49 - target_distance, and then the value is exact; a failing set
+returns some witness > 49 - target_distance (the reference's value after an
+early abort depends on thread timing, so only the decision is defined).
+Sampled screening reproduces the reference's splitmix64 message multiset for
+the same (set position, sample_seed), so a run without abort returns the same
+maximum as the reference.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import itertools
+import threading
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib
+from .tables import N_POINTS
+
+MAX_EXACT_K = 21
+MAX_SAMPLED_K = 49
+
+
+@dataclass
+class LaunchConfig:
+    """Launch shape of the persistent distance kernel."""
+
+    tail_rows: int = 0          # R; 0 = library default
+    enumeration: int = _lib.TG_ENUM_AUTO
+    variant: int = _lib.TG_VARIANT_AUTO
+    blocks_per_sm: int = 0
+    threads_per_block: int = 0
+
+
+def _require_cuda(device_id: int) -> None:
+    if not torch.cuda.is_available() or _lib.device_count() == 0:
+        raise RuntimeError("No CUDA GPU found.")
+    if device_id < 0 or device_id >= torch.cuda.device_count():
+        raise RuntimeError(f"CUDA device {device_id} does not exist")
+
+
+class ToricContext:
+    """One libtoric_b200 context (matrix tables on one device)."""
+
+    def __init__(self, device_id: int, M: np.ndarray):
+        _require_cuda(device_id)
+        lib = _lib.load()
+        m = np.ascontiguousarray(np.asarray(M, dtype=np.int32).reshape(N_POINTS, N_POINTS))
+        handle = ctypes.c_void_p()
+        _lib.check(
+            lib.tg_context_create(
+                device_id, m.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), ctypes.byref(handle)
+            ),
+            "tg_context_create",
+        )
+        self.handle = handle
+        self.device_id = device_id
+        flag = ctypes.c_int32(0)
+        _lib.check(lib.tg_context_is_toric(handle, ctypes.byref(flag)), "tg_context_is_toric")
+        self.is_toric = bool(flag.value)
+        self.sm_count = _lib.device_info(device_id)[0]
+
+    def close(self) -> None:
+        if self.handle:
+            _lib.load().tg_context_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):  # pragma: no cover - interpreter shutdown order
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def pack_sets(batched_indices) -> tuple[np.ndarray, np.ndarray, int]:
+    """Flattens a list of index lists into (flat int32, offsets int64, k_max)."""
+    lengths = np.fromiter((len(s) for s in batched_indices), dtype=np.int64,
+                          count=len(batched_indices))
+    offsets = np.zeros(len(batched_indices) + 1, dtype=np.int64)
+    np.cumsum(lengths, out=offsets[1:])
+    flat = np.fromiter(itertools.chain.from_iterable(batched_indices), dtype=np.int32,
+                       count=int(offsets[-1]))
+    k_max = int(lengths.max()) if len(lengths) else 0
+    return flat, offsets, k_max
+
+
+class DistanceRunner:
+    """Device-level max_zeros: inputs and outputs are torch CUDA tensors.
+
+    Owns a workspace that grows on demand and a CUDA stream; `run` enqueues
+    the prep, scan and persistent walk kernels without synchronising.
+    """
+
+    def __init__(self, ctx: ToricContext, config: LaunchConfig | None = None):
+        self.ctx = ctx
+        self.config = config or LaunchConfig()
+        self.device = torch.device("cuda", ctx.device_id)
+        self._ws: torch.Tensor | None = None
+        self.last_params: _lib.DistanceParams | None = None
+
+    def params(self, n_sets: int, k_max: int, target_distance: int, sample_count: int = 0,
+               sample_seed: int = 0) -> _lib.DistanceParams:
+        c = self.config
+        return _lib.DistanceParams(
+            n_sets=n_sets, k_max=k_max, tail_rows=c.tail_rows, enumeration=c.enumeration,
+            variant=c.variant, blocks_per_sm=c.blocks_per_sm,
+            threads_per_block=c.threads_per_block, target_distance=int(target_distance),
+            sample_count=int(sample_count), sample_seed=int(sample_seed) & (2**64 - 1),
+        )
+
+    def workspace(self, p: _lib.DistanceParams) -> torch.Tensor:
+        need = ctypes.c_size_t(0)
+        _lib.check(_lib.load().tg_distance_workspace_size(ctypes.byref(p), ctypes.byref(need)),
+                   "tg_distance_workspace_size")
+        if self._ws is None or self._ws.numel() < need.value:
+            self._ws = torch.empty(max(int(need.value), 256), dtype=torch.uint8,
+                                   device=self.device)
+        return self._ws
+
+    def run(self, p: _lib.DistanceParams, d_indices: torch.Tensor, d_offsets: torch.Tensor,
+            d_out: torch.Tensor, d_target: torch.Tensor | None = None,
+            d_set_ids: torch.Tensor | None = None, stream: torch.cuda.Stream | None = None,
+            workspace: torch.Tensor | None = None) -> None:
+        """Enqueues prepare + walk on `stream`."""
+        self.prepare(p, d_indices, d_offsets, d_out, d_target, d_set_ids, stream, workspace)
+        self.walk(p, d_out, stream, workspace)
+
+    def prepare(self, p: _lib.DistanceParams, d_indices: torch.Tensor, d_offsets: torch.Tensor,
+                d_out: torch.Tensor, d_target: torch.Tensor | None = None,
+                d_set_ids: torch.Tensor | None = None, stream: torch.cuda.Stream | None = None,
+                workspace: torch.Tensor | None = None) -> None:
+        ws = workspace if workspace is not None else self.workspace(p)
+        st = stream if stream is not None else torch.cuda.current_stream(self.device)
+        self.last_params = p
+        _lib.check(
+            _lib.load().tg_max_zeros_prepare(
+                self.ctx.handle, ctypes.byref(p), d_indices.data_ptr(), d_offsets.data_ptr(),
+                d_target.data_ptr() if d_target is not None else None,
+                d_set_ids.data_ptr() if d_set_ids is not None else None,
+                d_out.data_ptr(), ws.data_ptr(), ws.numel(), st.cuda_stream,
+            ),
+            "tg_max_zeros_prepare",
+        )
+
+    def walk(self, p: _lib.DistanceParams, d_out: torch.Tensor,
+             stream: torch.cuda.Stream | None = None,
+             workspace: torch.Tensor | None = None) -> None:
+        ws = workspace if workspace is not None else self.workspace(p)
+        st = stream if stream is not None else torch.cuda.current_stream(self.device)
+        _lib.check(
+            _lib.load().tg_max_zeros_walk(self.ctx.handle, ctypes.byref(p), d_out.data_ptr(),
+                                          ws.data_ptr(), ws.numel(), st.cuda_stream),
+            "tg_max_zeros_walk",
+        )
+
+    def status(self, p: _lib.DistanceParams, stream: torch.cuda.Stream) -> int:
+        s = ctypes.c_int32(0)
+        _lib.check(_lib.load().tg_distance_status(ctypes.byref(p), self._ws.data_ptr(),
+                                                  stream.cuda_stream, ctypes.byref(s)),
+                   "tg_distance_status")
+        return int(s.value)
+
+    def counters(self, stream: torch.cuda.Stream | None = None) -> tuple[int, int, float]:
+        """(tasks, codewords evaluated, reference messages 8^k-1 summed) of the last run."""
+        st = stream if stream is not None else torch.cuda.current_stream(self.device)
+        t, c, r = ctypes.c_uint64(0), ctypes.c_uint64(0), ctypes.c_double(0.0)
+        _lib.check(_lib.load().tg_distance_counters(ctypes.byref(self.last_params),
+                                                    self._ws.data_ptr(), st.cuda_stream,
+                                                    ctypes.byref(t), ctypes.byref(c),
+                                                    ctypes.byref(r)),
+                   "tg_distance_counters")
+        return int(t.value), int(c.value), float(r.value)
+
+
+class DistanceOracleCUDABP:
+    """Drop-in for the reference's DistanceOracleCUDABP (kernel_cuda_bp.py:246-323).
+
+    `max_zeros_batch` also accepts sets of different sizes in one call (they
+    share one persistent launch) and `target_distance` as a per-set sequence.
+    """
+
+    BLOCK_SIZE = 256  # kept for callers that read it; the B200 launch is persistent
+
+    def __init__(self, device_id: int, M: np.ndarray, config: LaunchConfig | None = None):
+        self.device_id = device_id
+        self.ctx = ToricContext(device_id, M)
+        self.runner = DistanceRunner(self.ctx, config)
+        self.device = self.runner.device
+        self._stream = torch.cuda.Stream(device=self.device)
+        self._lock = threading.Lock()
+
+    # -- reference API --------------------------------------------------------
+
+    def max_zeros(self, s_indices: list[int], target_distance: int) -> int:
+        k = len(s_indices)
+        if k == 0:
+            return 0
+        if k > MAX_EXACT_K:
+            raise ValueError("Exact CUDA-BP evaluation supports k <= 21")
+        return self._evaluate([list(s_indices)], target_distance, 0, 0)[0]
+
+    def max_zeros_batch(self, batched_indices, target_distance, sample_count: int = 0,
+                        sample_seed: int = 0) -> list[int]:
+        num_sets = len(batched_indices)
+        if num_sets == 0:
+            return []
+        return self._evaluate(batched_indices, target_distance, sample_count, sample_seed)
+
+    def min_distance(self, s_indices: list[int], target_distance: int = 1) -> int:
+        """49 - max_zeros (the helper of kernel backup.py:161-163)."""
+        return N_POINTS - self.max_zeros(s_indices, target_distance)
+
+    # -- implementation -------------------------------------------------------
+
+    def _evaluate(self, batched_indices, target_distance, sample_count, sample_seed) -> list[int]:
+        flat, offsets, k_max = pack_sets(batched_indices)
+        if k_max > MAX_SAMPLED_K:
+            raise ValueError("CUDA-BP bit-parallel kernel supports k <= 49")
+        if sample_count <= 0 and k_max > MAX_EXACT_K:
+            raise ValueError("Exact CUDA-BP batch evaluation supports k <= 21")
+        if flat.size and (int(flat.min()) < 0 or int(flat.max()) >= N_POINTS):
+            raise ValueError("exponent indices must lie in 0..48")
+        n = len(batched_indices)
+        per_set_td = not np.isscalar(target_distance)
+        td_arr = None
+        if per_set_td:
+            td_arr = np.asarray(target_distance, dtype=np.int32)
+            if td_arr.shape != (n,):
+                raise ValueError("target_distance must be an int or one value per set")
+        with self._lock, torch.cuda.device(self.device):
+            s = self._stream
+            with torch.cuda.stream(s):
+                d_idx = torch.from_numpy(flat if flat.size else np.zeros(1, np.int32)).pin_memory()
+                d_idx = d_idx.to(self.device, non_blocking=True)
+                d_off = torch.from_numpy(offsets).pin_memory().to(self.device, non_blocking=True)
+                d_td = None
+                if td_arr is not None:
+                    d_td = torch.from_numpy(td_arr).pin_memory().to(self.device, non_blocking=True)
+                d_out = torch.empty(n, dtype=torch.int32, device=self.device)
+                p = self.runner.params(n, k_max, 0 if per_set_td else int(target_distance),
+                                       sample_count if sample_count > 0 else 0, sample_seed)
+                self.runner.run(p, d_idx, d_off, d_out, d_target=d_td, stream=s)
+                h_out = torch.empty(n, dtype=torch.int32, pin_memory=True)
+                h_out.copy_(d_out, non_blocking=True)
+            status = self.runner.status(p, s)  # synchronises the stream
+        if status != _lib.TG_OK:
+            _lib.check(status, "max_zeros_batch (device)")
+        return h_out.tolist()
+
+
+def init_cuda_oracles_bp(M: np.ndarray) -> tuple[list[DistanceOracleCUDABP], int]:
+    """One oracle per visible GPU and the SM count of device 0
+    (kernel_cuda_bp.py:330-347)."""
+    if not torch.cuda.is_available():
+        raise RuntimeError("No CUDA GPU found.")
+    n = _lib.device_count()
+    if n == 0:
+        raise RuntimeError("No CUDA GPU found.")
+    oracles: list[DistanceOracleCUDABP] = []
+    sm_count = 40
+    for i in range(n):
+        sm_i, _, _, name = _lib.device_info(i)
+        print(f"[CUDA-B200] Device {i}: {name}  ({sm_i} SMs)")
+        if i == 0:
+            sm_count = sm_i
+        oracles.append(DistanceOracleCUDABP(i, M))
+    return oracles, sm_count

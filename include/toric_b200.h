@@ -1,0 +1,210 @@
+/*
+ * toric_b200.h — C ABI of libtoric_b200.so, the sm_100a implementation of the
+ * GF(8) generalized-toric-code hot path:
+ *
+ *   - max_zeros: for a code spanned by the rows M[S] of the 49x49 evaluation
+ *     matrix, the largest number of zero coordinates of a nonzero codeword
+ *     (minimum distance d = 49 - max_zeros), with the reference's early-exit
+ *     threshold and its splitmix64 sampled screening mode;
+ *   - the AGL2(F7) canonical form of an exponent set (anchored minimum, with
+ *     the reference's packed 6-bit key for k <= 16 and a 49-bit mask for any k);
+ *   - a device hash set that deduplicates canonical keys;
+ *   - a device-resident serving loop (continuous batching of max_zeros
+ *     requests with per-request thresholds and canonical dedup).
+ *
+ * Conventions
+ *   - Every entry point returns a status code (TG_OK == 0); no exception ever
+ *     crosses the boundary.  tg_status_string() names a code and
+ *     tg_last_error() gives the message of the calling thread's last failure.
+ *   - Pointers named d_* are device pointers on the context's device; h_*
+ *     are host pointers.  `stream` is a cudaStream_t passed as void*
+ *     (NULL = legacy default stream).  Work is enqueued on `stream` and the
+ *     call returns without synchronising unless stated otherwise.
+ *   - The library owns only its small per-context constant tables.  All
+ *     per-call scratch lives in caller-provided workspaces, so the calls are
+ *     re-entrant per stream and can be captured into CUDA graphs.
+ *   - Exponent index i in 0..48 is the point (a, b) = (i / 7, i % 7) of Z_7^2;
+ *     row i of M is the monomial x^a y^b evaluated at the 49 torus points.
+ */
+#ifndef TORIC_B200_H
+#define TORIC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TG_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+  TG_OK = 0,
+  TG_ERR_INVALID_ARGUMENT = 1, /* bad size, k out of range, NULL pointer   */
+  TG_ERR_CUDA = 2,             /* a CUDA runtime call failed               */
+  TG_ERR_WORKSPACE = 3,        /* workspace smaller than required          */
+  TG_ERR_NO_DEVICE = 4,        /* no CUDA device / bad device ordinal      */
+  TG_ERR_CAPACITY = 5,         /* hash table or serving ring full          */
+  TG_ERR_TIMEOUT = 6,          /* a bounded device wait gave up            */
+  TG_ERR_BAD_INPUT = 7,        /* index outside 0..48 found on the device  */
+  TG_ERR_STATE = 8             /* call not valid in the object's state     */
+};
+
+typedef struct tg_context tg_context;
+
+/* Name of a status code (static string). */
+const char* tg_status_string(int status);
+/* Message of the calling thread's most recent failed call (static per thread). */
+const char* tg_last_error(void);
+/* TG_ABI_VERSION of the loaded library. */
+int tg_abi_version(void);
+
+/* ---- device and context ------------------------------------------------ */
+
+/* Number of visible CUDA devices (0 when none). */
+int tg_device_count(int32_t* h_count);
+
+/* SM count, compute capability and name of a device. */
+int tg_device_info(int device, int32_t* h_sm_count, int32_t* h_cc_major,
+                   int32_t* h_cc_minor, char* h_name, int32_t name_len);
+
+/* Creates a context on `device` from the 49x49 evaluation matrix M (host,
+ * row-major int32, entries 0..7).  Replaces DistanceOracleCUDABP.__init__
+ * (kernel_cuda_bp.py:251-258) and CanonicalOracle.__init__
+ * (kernel_canon.py:137-148): uploads the matrix tables and the GL2(F7) point
+ * permutations once.  When M equals the toric matrix of precompute.py:32-43
+ * the context enables the torus-orbit enumeration (see tg_distance_params). */
+int tg_context_create(int device, const int32_t* h_M, tg_context** out_ctx);
+int tg_context_destroy(tg_context* ctx);
+/* 1 when the context's M is the toric evaluation matrix, else 0. */
+int tg_context_is_toric(const tg_context* ctx, int32_t* h_is_toric);
+
+/* ---- max_zeros (exact and sampled) -------------------------------------- */
+
+enum {
+  TG_ENUM_AUTO = 0,       /* orbit when the context is toric, else projective */
+  TG_ENUM_PROJECTIVE = 1, /* messages whose first nonzero coefficient is 1    */
+  TG_ENUM_ORBIT = 2       /* projective + torus-orbit normalisation (toric M) */
+};
+enum {
+  TG_VARIANT_AUTO = 0,      /* histogram when the context is toric            */
+  TG_VARIANT_HISTOGRAM = 1, /* last row via an 8-bin zero histogram           */
+  TG_VARIANT_DIRECT = 2     /* one popcount pair per codeword                 */
+};
+
+typedef struct tg_distance_params {
+  int32_t n_sets;          /* number of codes in the batch (>= 0)            */
+  int32_t k_max;           /* largest k in the batch (exact: <= 21, sampled: <= 49) */
+  int32_t tail_rows;       /* R: rows walked inside one task; 0 = default    */
+  int32_t enumeration;     /* TG_ENUM_*                                      */
+  int32_t variant;         /* TG_VARIANT_*                                   */
+  int32_t blocks_per_sm;   /* persistent CTAs per SM; 0 = default            */
+  int32_t threads_per_block; /* 0 = default (128)                            */
+  int32_t target_distance; /* used for every set when d_target is NULL       */
+  int64_t sample_count;    /* 0 = exact; > 0 = reference sampled screening   */
+  uint64_t sample_seed;    /* splitmix64 seed of the sampled mode            */
+} tg_distance_params;
+
+/* Bytes of workspace tg_max_zeros needs for these parameters. */
+int tg_distance_workspace_size(const tg_distance_params* p, size_t* h_bytes);
+
+/* max_zeros of every set of a batch of mixed sizes, in one persistent launch.
+ * Replaces DistanceOracleCUDABP.max_zeros_batch (kernel_cuda_bp.py:290-323,
+ * kernel eval_min_distance_batch_bp :146-238) and DistanceOracle.max_zeros_batch
+ * (kernel.py:276-323); a one-set batch replaces max_zeros
+ * (kernel_cuda_bp.py:266-288, kernel.py:241-274).
+ *   d_indices  flat exponent indices of all sets (int32, 0..48)
+ *   d_offsets  n_sets+1 int64 offsets into d_indices (set s = [off[s], off[s+1]))
+ *   d_target   per-set target_distance (int32) or NULL (p->target_distance)
+ *   d_set_ids  per-set sampling id (the reference's blockIdx.x) or NULL (= s)
+ *   d_out      per-set max_zeros (int32).  A set passes iff out <= 49 - td, and
+ *              then out is exact; a failing set returns a witness > 49 - td.
+ * The workspace must be 256-byte aligned and hold tg_distance_workspace_size
+ * bytes.  Indices outside 0..48 make the call report TG_ERR_BAD_INPUT through
+ * tg_distance_status() after the stream reaches it. */
+int tg_max_zeros(tg_context* ctx, const tg_distance_params* p,
+                 const int32_t* d_indices, const int64_t* d_offsets,
+                 const int32_t* d_target, const int32_t* d_set_ids,
+                 int32_t* d_out, void* d_workspace, size_t workspace_bytes,
+                 void* stream);
+
+/* The two halves of tg_max_zeros, for callers that time or capture them
+ * separately: _prepare validates the sets, orders rows, builds the bit-sliced
+ * bases and the task table (prep + scan kernels); _walk runs the persistent
+ * enumeration kernel over the prepared tasks and writes d_out.  Same
+ * arguments and workspace as tg_max_zeros; d_out of _prepare receives the
+ * values of sets decided without enumeration (k <= 1, repeated rows). */
+int tg_max_zeros_prepare(tg_context* ctx, const tg_distance_params* p,
+                         const int32_t* d_indices, const int64_t* d_offsets,
+                         const int32_t* d_target, const int32_t* d_set_ids,
+                         int32_t* d_out, void* d_workspace,
+                         size_t workspace_bytes, void* stream);
+int tg_max_zeros_walk(tg_context* ctx, const tg_distance_params* p,
+                      int32_t* d_out, void* d_workspace, size_t workspace_bytes,
+                      void* stream);
+
+/* Device status word of the last tg_max_zeros run on this workspace
+ * (synchronises `stream`): TG_OK or TG_ERR_BAD_INPUT. */
+int tg_distance_status(const tg_distance_params* p, const void* d_workspace,
+                       void* stream, int32_t* h_status);
+
+/* Work accounting of the last run on this workspace (synchronises `stream`):
+ * tasks launched, codewords evaluated (sum over tasks) and the
+ * reference-equivalent message count sum(8^k - 1) over exact sets. */
+int tg_distance_counters(const tg_distance_params* p, const void* d_workspace,
+                         void* stream, uint64_t* h_tasks,
+                         uint64_t* h_codewords, double* h_reference_messages);
+
+/* ---- canonical forms ---------------------------------------------------- */
+
+/* Canonical form of n exponent sets given as rows of a (n, k) int32 matrix.
+ * Replaces CanonicalOracle.compute (kernel_canon.py:151-176; kernel
+ * canonical_forms :44-129) and canonical_forms_batch
+ * (champion_search_canonical.py:115-140).
+ *   d_out_mask  canonical 49-bit mask (bit i = exponent index i): the
+ *               smallest mask of an AGL2(F7) image of the set that contains
+ *               the origin.  Defined for every k in 1..49.
+ *   d_out_key_lo/hi  the reference's packed key (6 bits per sorted index,
+ *               index 0 skipped for k >= 11) for k <= 16, else all ones.
+ * Rows with repeated or out-of-range indices get mask 0 and key all ones and
+ * raise TG_ERR_BAD_INPUT in *d_status (int32, may be NULL). */
+int tg_canonical_sets(tg_context* ctx, const int32_t* d_sets, int32_t n,
+                      int32_t k, uint64_t* d_out_mask, uint64_t* d_out_key_lo,
+                      uint64_t* d_out_key_hi, int32_t* d_status, void* stream);
+
+/* Same for sets given as 49-bit masks (popcount 1..49; 0 -> mask 0). */
+int tg_canonical_masks(tg_context* ctx, const uint64_t* d_masks, int32_t n,
+                       uint64_t* d_out_mask, uint64_t* d_out_key_lo,
+                       uint64_t* d_out_key_hi, void* stream);
+
+/* ---- device hash set (canonical dedup) ----------------------------------- */
+
+/* Bytes of a hash set with `capacity` slots (power of two >= 64). */
+int tg_hashset_bytes(int64_t capacity, size_t* h_bytes);
+/* Empties a hash set. */
+int tg_hashset_clear(void* d_table, int64_t capacity, void* stream);
+/* Inserts n 64-bit keys (any value but all ones).  d_is_new[i] = 1 iff key i
+ * was absent before this call and i is its first index in this call — the
+ * semantics of the reference's `seen` set walk in
+ * champion_search_canonical.py:337-345.  `call_id` must grow from call to
+ * call on one table (1, 2, ...).  d_n_new (may be NULL) receives the count.
+ * A table fuller than half its capacity sets TG_ERR_CAPACITY in *d_status. */
+int tg_hashset_insert(void* d_table, int64_t capacity, const uint64_t* d_keys,
+                      int32_t n, uint32_t call_id, uint8_t* d_is_new,
+                      int32_t* d_n_new, int32_t* d_status, void* stream);
+
+/* ---- integer pipe throughput (roofline denominators) --------------------- */
+
+/* Measures per-SM issue rates (operations per SM per clock) of the integer
+ * instructions the distance kernel uses: out[0] LOP3, out[1] POPC, out[2]
+ * IADD3, out[3] fused add+max, out[4] LOP3+POPC interleaved 1:1 (ops of both
+ * kinds), out[5] the SM clock in MHz seen during the run.  Needs
+ * d_scratch of 1 MiB.  Synchronises. */
+int tg_measure_int_pipes(int device, void* d_scratch, double* h_out6);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TORIC_B200_H */
