@@ -1,0 +1,129 @@
+"""Bit-exact parity with the reference's own CUDA kernels on the B200.
+
+oracle/build_ref.py compiles the reference's kernel source strings
+(kernel_cuda_bp.py, kernel_canon.py) for sm_100a into
+oracle/_ref/libref_kernels.so, launched with the reference wrappers' geometry
+by oracle/ref_harness.cu.  These tests run both implementations on the same
+inputs.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import random
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ROOT = Path(__file__).resolve().parents[1]
+REF_LIB = ROOT / "oracle" / "_ref" / "libref_kernels.so"
+N = 49
+
+
+@pytest.fixture(scope="module")
+def ref():
+    if not REF_LIB.exists():
+        pytest.skip("oracle/_ref/libref_kernels.so not built (needs the reference checkout)")
+    lib = ctypes.CDLL(str(REF_LIB))
+    vp = ctypes.c_void_p
+    lib.ref_bp_batch.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                 ctypes.c_longlong, ctypes.c_ulonglong, vp, vp]
+    lib.ref_bp_single.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, vp, vp]
+    lib.ref_canon.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int, ctypes.c_int, vp]
+    return lib
+
+
+@pytest.fixture(scope="module")
+def dev_M(M):
+    import torch
+
+    return torch.from_numpy(np.ascontiguousarray(M.astype(np.int32))).cuda()
+
+
+def ref_batch(ref, dev_M, sets, td, sample_count=0, seed=0):
+    import torch
+
+    k = len(sets[0])
+    flat = torch.tensor([i for s in sets for i in s], dtype=torch.int32).cuda()
+    out = torch.zeros(len(sets), dtype=torch.int32).cuda()
+    rc = ref.ref_bp_batch(dev_M.data_ptr(), flat.data_ptr(), k, N - td, len(sets), sample_count,
+                          seed & (2**64 - 1), out.data_ptr(), None)
+    assert rc == 0
+    torch.cuda.synchronize()
+    return out.cpu().tolist()
+
+
+@pytest.mark.parametrize("k", [2, 3, 5, 7, 8, 9])
+def test_exact_batch_vs_reference_kernel(ref, dev_M, gpu_oracle, k):
+    rng = random.Random(500 + k)
+    sets = [sorted(rng.sample(range(N), k)) for _ in range(48)]
+    assert gpu_oracle.max_zeros_batch(sets, 1) == ref_batch(ref, dev_M, sets, 1)
+
+
+def test_config_c1_vs_reference_kernel(ref, dev_M, gpu_oracle):
+    rng = np.random.default_rng(1)
+    sets = [sorted(rng.choice(N, 8, replace=False).tolist()) for _ in range(64)]
+    assert gpu_oracle.max_zeros_batch(sets, 1) == ref_batch(ref, dev_M, sets, 1)
+
+
+@pytest.mark.parametrize("k,td", [(6, 38), (7, 36), (8, 33)])
+def test_threshold_decisions_vs_reference_kernel(ref, dev_M, gpu_oracle, k, td):
+    rng = random.Random(900 + k)
+    sets = [sorted(rng.sample(range(N), k)) for _ in range(64)]
+    exact = ref_batch(ref, dev_M, sets, 1)
+    ours = gpu_oracle.max_zeros_batch(sets, td)
+    theirs = ref_batch(ref, dev_M, sets, td)
+    tmax = N - td
+    for e, a, b in zip(exact, ours, theirs):
+        assert (a > tmax) == (b > tmax) == (e > tmax)
+        if e <= tmax:
+            assert a == b == e
+
+
+@pytest.mark.parametrize("k", [4, 11, 15, 21, 22, 33, 49])
+def test_sampled_vs_reference_kernel(ref, dev_M, gpu_oracle, k):
+    rng = random.Random(700 + k)
+    sets = [sorted(rng.sample(range(N), k)) for _ in range(40)]
+    for seed in (1, 2**40 + 3):
+        want = ref_batch(ref, dev_M, sets, 1, sample_count=20_000, seed=seed)
+        got = gpu_oracle.max_zeros_batch(sets, 1, sample_count=20_000, sample_seed=seed)
+        assert got == want
+
+
+def test_single_set_kernel(ref, dev_M, gpu_oracle):
+    import torch
+
+    rng = random.Random(31)
+    for k in (1, 3, 6, 8):
+        s = sorted(rng.sample(range(N), k))
+        out = torch.zeros(1, dtype=torch.int32).cuda()
+        d_s = torch.tensor(s, dtype=torch.int32).cuda()
+        assert ref.ref_bp_single(dev_M.data_ptr(), d_s.data_ptr(), k, N - 1, out.data_ptr(),
+                                 None) == 0
+        torch.cuda.synchronize()
+        assert gpu_oracle.max_zeros(s, 1) == int(out.item())
+
+
+@pytest.mark.parametrize("k", [1, 2, 5, 8, 10, 11, 12, 14, 16])
+def test_canonical_vs_reference_kernel(ref, canon_oracle, k):
+    import torch
+
+    from generalized_toric_gpu_search_b200.tables import precompute_gl2_perms, rel_table
+
+    rng = random.Random(300 + k)
+    sets = np.array([sorted(rng.sample(range(N), k)) for _ in range(200)], dtype=np.int32)
+    d_sets = torch.from_numpy(sets).cuda()
+    perms = torch.from_numpy(precompute_gl2_perms()).cuda()
+    rel = torch.from_numpy(rel_table()).cuda()
+    lo = torch.full((len(sets),), -1, dtype=torch.int64).cuda()
+    hi = torch.zeros(len(sets), dtype=torch.int64).cuda()
+    assert ref.ref_canon(d_sets.data_ptr(), perms.data_ptr(), rel.data_ptr(), lo.data_ptr(),
+                         hi.data_ptr(), len(sets), k, None) == 0
+    torch.cuda.synchronize()
+    lo_u = lo.cpu().numpy().view(np.uint64)
+    hi_u = hi.cpu().numpy().view(np.uint64)
+    want = [int(a) | (int(b) << 64) for a, b in zip(lo_u, hi_u)]
+    assert [int(x) for x in canon_oracle.compute(sets)] == want
