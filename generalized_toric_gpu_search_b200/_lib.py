@@ -57,6 +57,9 @@ SIGNATURES: dict[str, tuple] = {
          c_size_t, c_void_p],
     ),
     "tg_max_zeros_walk": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
+    "tg_max_zeros_noalloc": (
+        c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]
+    ),
     "tg_distance_status": (c_int, [c_void_p, c_void_p, c_void_p, POINTER(c_int32)]),
     "tg_distance_counters": (
         c_int,

@@ -3,6 +3,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -449,3 +450,71 @@ int tg_measure_int_pipes(int device, void* d_scratch, double* h_out6) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Zero-allocation max_zeros: the workspace is a scratch array compiled into
+// the library instead of caller memory.
+// ---------------------------------------------------------------------------
+
+namespace tg {
+
+constexpr size_t kStaticWorkspaceBytes = size_t(TG_STATIC_WORKSPACE_BYTES);
+
+// One copy per device that loads the library, alive until the process exits.
+static __device__ __align__(256) uint8_t g_static_workspace[kStaticWorkspaceBytes];
+
+// Device address of g_static_workspace per device ordinal.  In host code the
+// symbol itself is only a host-side stand-in, so the address is looked up
+// once per device, with that device current, and cached here.
+static void* g_static_workspace_addr[64] = {nullptr};
+static std::mutex g_static_workspace_mu;
+
+static int static_workspace_address(int device, void** out) {
+  if (device < 0 || device >= 64) {
+    set_last_error("device %d has no static workspace slot", device);
+    return TG_ERR_NO_DEVICE;
+  }
+  std::lock_guard<std::mutex> lock(g_static_workspace_mu);
+  if (!g_static_workspace_addr[device]) {
+    void* addr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&addr, g_static_workspace);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_static_workspace)");
+    g_static_workspace_addr[device] = addr;
+  }
+  *out = g_static_workspace_addr[device];
+  return TG_OK;
+}
+
+}  // namespace tg
+
+extern "C" int tg_max_zeros_noalloc(tg_context* ctx, const tg_distance_params* p,
+                                    const int32_t* d_indices, const int64_t* d_offsets,
+                                    const int32_t* d_target, const int32_t* d_set_ids,
+                                    int32_t* d_out, void* stream) {
+  if (!ctx) return invalid("tg_max_zeros_noalloc: NULL context");
+  int st = check_distance_params(p);
+  if (st) return st;
+  if (p->n_sets == 0) return TG_OK;
+  const size_t need = ws_layout(*p).total;
+  if (need > kStaticWorkspaceBytes) {
+    set_last_error("tg_max_zeros_noalloc: this batch needs %zu bytes of workspace but the "
+                   "static workspace holds %zu; split the batch or use tg_max_zeros",
+                   need, kStaticWorkspaceBytes);
+    return TG_ERR_WORKSPACE;
+  }
+  DeviceGuard g(ctx->device);
+  if (g.error() != cudaSuccess) return cuda_fail(g.error(), "cudaSetDevice");
+  void* ws = nullptr;
+  st = static_workspace_address(ctx->device, &ws);
+  if (st) return st;
+  DistArgs a;
+  st = bind_distance(ctx, p, d_indices, d_offsets, d_target, d_set_ids, d_out, ws,
+                     kStaticWorkspaceBytes, true, a);
+  if (st) return st;
+  const cudaStream_t s = static_cast<cudaStream_t>(stream);
+  st = run_prepare(a, s);
+  if (st) return st;
+  int bps, tpb;
+  launch_shape(p, &bps, &tpb);
+  return run_walk(a, ctx->sm_count, bps, tpb, s);
+}

@@ -144,6 +144,30 @@ int tg_max_zeros_walk(tg_context* ctx, const tg_distance_params* p,
                       int32_t* d_out, void* d_workspace, size_t workspace_bytes,
                       void* stream);
 
+/* Size of the library-owned scratch area tg_max_zeros_noalloc works in. */
+#define TG_STATIC_WORKSPACE_BYTES (16u << 20)
+
+/* tg_max_zeros for callers that must not allocate device memory.
+ * No counterpart in the reference (its oracles allocate per call through
+ * CuPy).  Meant for hosts where device memory is carved out up front or owned
+ * by another allocator -- an application that hands this library a fixed
+ * pool, a plugin whose host forbids cudaMalloc after start-up, a latency-bound
+ * loop that cannot afford an allocation's implicit synchronisation.  It takes
+ * the same inputs and writes the same d_out as tg_max_zeros but runs in a
+ * TG_STATIC_WORKSPACE_BYTES scratch array compiled into the library (held on
+ * every device that loads it) and allocates nothing.  The first call on a
+ * device looks the array's device address up (cudaGetSymbolAddress), so make
+ * that first call before any stream capture on that device.  Batches whose
+ * tg_distance_workspace_size exceeds the array are refused with
+ * TG_ERR_WORKSPACE.  All calls share the one array: calls that may overlap on
+ * the GPU (different streams, or different host threads) race and must be
+ * serialised by the caller.  Sets with indices outside 0..48 come back as 0;
+ * there is no status query for this path. */
+int tg_max_zeros_noalloc(tg_context* ctx, const tg_distance_params* p,
+                         const int32_t* d_indices, const int64_t* d_offsets,
+                         const int32_t* d_target, const int32_t* d_set_ids,
+                         int32_t* d_out, void* stream);
+
 /* Device status word of the last tg_max_zeros run on this workspace
  * (synchronises `stream`): TG_OK or TG_ERR_BAD_INPUT. */
 int tg_distance_status(const tg_distance_params* p, const void* d_workspace,
