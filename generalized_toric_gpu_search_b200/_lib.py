@@ -79,7 +79,51 @@ SIGNATURES: dict[str, tuple] = {
         [c_void_p, c_int64, c_void_p, c_int32, c_uint32, c_void_p, c_void_p, c_void_p, c_void_p],
     ),
     "tg_measure_int_pipes": (c_int, [c_int, c_void_p, POINTER(c_double)]),
+    "tg_server_layout": (
+        c_int, [c_void_p, c_void_p, POINTER(c_int32), POINTER(c_size_t), POINTER(c_size_t)]
+    ),
+    "tg_server_create": (
+        c_int, [c_void_p, c_void_p, c_void_p, c_size_t, c_void_p, c_size_t, POINTER(c_void_p)]
+    ),
+    "tg_server_submit": (c_int, [c_void_p, c_void_p, c_int32, c_int32, POINTER(c_uint32)]),
+    "tg_server_pump": (c_int, [c_void_p, POINTER(c_int32)]),
+    "tg_server_poll": (c_int, [c_void_p, c_void_p, c_int32, POINTER(c_int32)]),
+    "tg_server_stats": (c_int, [c_void_p, POINTER(c_uint64)]),
+    "tg_server_destroy": (c_int, [c_void_p]),
 }
+
+TG_RESULT_PASS = 1
+TG_RESULT_FAIL = 2
+TG_RESULT_DEDUP = 4
+TG_RESULT_BAD_INPUT = 8
+
+
+class ServerParams(ctypes.Structure):
+    """Mirror of tg_server_params."""
+
+    _fields_ = [
+        ("max_slots", c_int32),
+        ("k_max", c_int32),
+        ("tail_rows", c_int32),
+        ("blocks_per_sm", c_int32),
+        ("idle_us", c_int32),
+        ("life_ms", c_int32),
+        ("table_capacity", c_int64),
+        ("memory_fraction", c_double),
+    ]
+
+
+class ServerResult(ctypes.Structure):
+    """Mirror of tg_server_result."""
+
+    _fields_ = [
+        ("id", c_uint32),
+        ("max_zeros", c_int32),
+        ("flags", c_int32),
+        ("pad", c_int32),
+        ("t_admit_ns", c_uint64),
+        ("t_done_ns", c_uint64),
+    ]
 
 
 class DistanceParams(ctypes.Structure):

@@ -15,7 +15,7 @@ PKG_DIR = Path(__file__).resolve().parent
 CSRC = PKG_DIR / "csrc"
 LIB_NAME = "libtoric_b200.so"
 LIB_PATH = PKG_DIR / LIB_NAME
-SOURCES = ["abi.cu", "distance.cu", "canonical.cu", "intpeak.cu"]
+SOURCES = ["abi.cu", "distance.cu", "canonical.cu", "intpeak.cu", "server.cu"]
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

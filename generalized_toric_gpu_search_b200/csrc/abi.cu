@@ -7,16 +7,10 @@
 #include <vector>
 
 #include "common.cuh"
+#include "context.cuh"
 #include "canonical.cuh"
 #include "distance.cuh"
 
-struct tg_context {
-  int device;
-  int sm_count;
-  int is_toric;
-  uint8_t* d_M;    // 49 x 49
-  uint8_t* d_gl2;  // 2016 x 49
-};
 
 namespace tg {
 

@@ -23,7 +23,6 @@ namespace tg {
 
 constexpr int kCanonTPB = 256;
 constexpr int kGl2Bytes = kGl2Order * kN;          // 98,784
-constexpr uint64_t kRep7 = 0x0000040810204081ull;  // bits 0, 7, ..., 42
 
 struct CanonArgs {
   const int32_t* sets;    // (n, k) rows, or NULL
@@ -36,43 +35,6 @@ struct CanonArgs {
   int32_t* status;
   const uint8_t* gl2;
 };
-
-// Translation of a 49-bit torus mask by -(qa, qb): columns rotate right by qb
-// inside each row of 7, rows rotate down by qa.
-__device__ __forceinline__ uint64_t torus_shift(uint64_t m, int qa, int qb) {
-  const uint64_t low = ((1ull << (7 - qb)) - 1ull) * kRep7;
-  const uint64_t cr = ((m >> qb) & low) | ((m << (7 - qb)) & (kMask49 & ~low));
-  const int r = 7 * qa;
-  return ((cr >> r) | (cr << (kN - r))) & kMask49;
-}
-
-__device__ __forceinline__ void key_from_mask(uint64_t m, uint64_t& lo, uint64_t& hi) {
-  const int k = __popcll(m);
-  if (k < 1 || k > 16) {
-    lo = ~0ull;
-    hi = ~0ull;
-    return;
-  }
-  const int pf = k <= 10 ? 0 : 1;
-  lo = 0ull;
-  hi = 0ull;
-  int i = 0;
-  while (m) {
-    const int idx = __ffsll(static_cast<long long>(m)) - 1;
-    m &= m - 1ull;
-    if (i >= pf) {
-      const int off = 6 * (i - pf);
-      const uint64_t v = uint64_t(idx);
-      if (off < 64) {
-        lo |= v << off;
-        if (off + 6 > 64) hi |= v >> (64 - off);
-      } else {
-        hi |= v << (off - 64);
-      }
-    }
-    ++i;
-  }
-}
 
 __global__ void __launch_bounds__(kCanonTPB, 2) canon_kernel(CanonArgs a) {
   extern __shared__ __align__(16) uint8_t s_perm[];

@@ -85,12 +85,38 @@ __device__ __forceinline__ int ld_flag(const int32_t* p) {
   return *reinterpret_cast<const volatile int32_t*>(p);
 }
 
+// Loads of data that no thread writes during the kernel (kCG = false, the
+// non-coherent read-only path) or that other SMs may rewrite while the kernel
+// runs (kCG = true: cached in L2 only, so never a stale L1 line).
+template <bool kCG>
+__device__ __forceinline__ uint64_t ld_u64(const uint64_t* p) {
+  if (kCG) return __ldcg(reinterpret_cast<const unsigned long long*>(p));
+  return __ldg(reinterpret_cast<const unsigned long long*>(p));
+}
+
+template <bool kCG>
+__device__ __forceinline__ uint32_t ld_u32(const uint32_t* p) {
+  return kCG ? __ldcg(p) : __ldg(p);
+}
+
+template <bool kCG>
+__device__ __forceinline__ V6 v6_load(const V6* p) {
+  const uint4* q = reinterpret_cast<const uint4*>(p);
+  const uint4 a = kCG ? __ldcg(q) : __ldg(q);
+  const uint4 b = kCG ? __ldcg(q + 1) : __ldg(q + 1);
+  V6 v;
+  v.l0 = a.x; v.l1 = a.y; v.l2 = a.z; v.h0 = a.w;
+  v.h1 = b.x; v.h2 = b.y; v.pad0 = 0u; v.pad1 = 0u;
+  return v;
+}
+
 // Index of the last element of sorted a[0..n) that is <= x (a[0] <= x).
+template <bool kCG = false>
 __device__ __forceinline__ int last_le(const uint64_t* a, int n, uint64_t x) {
   int lo = 0, hi = n - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
-    if (__ldg(a + mid) <= x) lo = mid; else hi = mid - 1;
+    if (ld_u64<kCG>(a + mid) <= x) lo = mid; else hi = mid - 1;
   }
   return lo;
 }
@@ -108,6 +134,45 @@ __host__ __device__ __forceinline__ uint64_t mod_mersenne(uint64_t x, int m) {
   const uint64_t M = (1ull << m) - 1ull;
   while (x > M) x = (x & M) + (x >> m);
   return x == M ? 0ull : x;
+}
+
+constexpr uint64_t kRep7 = 0x0000040810204081ull;  // bits 0, 7, ..., 42
+
+// Translation of a 49-bit torus mask by -(qa, qb): columns rotate right by qb
+// inside each row of 7, rows rotate down by qa.
+__device__ __forceinline__ uint64_t torus_shift(uint64_t m, int qa, int qb) {
+  const uint64_t low = ((1ull << (7 - qb)) - 1ull) * kRep7;
+  const uint64_t cr = ((m >> qb) & low) | ((m << (7 - qb)) & (kMask49 & ~low));
+  const int r = 7 * qa;
+  return ((cr >> r) | (cr << (kN - r))) & kMask49;
+}
+
+__device__ __forceinline__ void key_from_mask(uint64_t m, uint64_t& lo, uint64_t& hi) {
+  const int k = __popcll(m);
+  if (k < 1 || k > 16) {
+    lo = ~0ull;
+    hi = ~0ull;
+    return;
+  }
+  const int pf = k <= 10 ? 0 : 1;
+  lo = 0ull;
+  hi = 0ull;
+  int i = 0;
+  while (m) {
+    const int idx = __ffsll(static_cast<long long>(m)) - 1;
+    m &= m - 1ull;
+    if (i >= pf) {
+      const int off = 6 * (i - pf);
+      const uint64_t v = uint64_t(idx);
+      if (off < 64) {
+        lo |= v << off;
+        if (off + 6 > 64) hi |= v >> (64 - off);
+      } else {
+        hi |= v << (off - 64);
+      }
+    }
+    ++i;
+  }
 }
 
 // Context tables shared by the kernels (device memory of one context).

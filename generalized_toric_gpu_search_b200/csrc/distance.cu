@@ -37,6 +37,7 @@
 
 #include "common.cuh"
 #include "distance.cuh"
+#include "serve.cuh"
 
 namespace tg {
 
@@ -149,6 +150,136 @@ __device__ __forceinline__ V6 ballot_planes(int lane, uint32_t v_lo, uint32_t v_
   return r;
 }
 
+struct PrepResult {
+  int result;        // max_zeros when decided without enumeration
+  uint64_t n_tasks;  // tasks of the walk (0 when decided)
+  int n_pat;
+  int R;
+  int H;
+};
+
+// Warp-level preparation of one code whose k (< 32) valid exponent indices
+// are in s_idx[0..k): repeated rows and k <= 1 are decided directly; else
+// the rows are ordered (leading head rows in general position for the orbit
+// enumeration), the bit-sliced basis B[r*3 + t] = alpha^t row_r (divided
+// coordinate-wise by the last row for the histogram variant) and the pattern
+// table (cum, info) are written.  s_row is per-warp scratch of 32 ints.
+__device__ PrepResult prep_code(int lane, int k, const int* s_idx, int* s_row, int R_param,
+                                int enumeration, int variant, const uint8_t* M, V6* B,
+                                uint64_t* cum, uint32_t* info) {
+  PrepResult out{0, 0ull, 0, 0, 0};
+  const int my = lane < k ? s_idx[lane] : -1 - lane;
+  bool dup = false;
+  if (k > 1) {
+    const unsigned act = __ballot_sync(0xffffffffu, lane < k);
+    const unsigned m = __match_any_sync(0xffffffffu, my);
+    dup = __any_sync(0xffffffffu, (act >> lane & 1u) && __popc(m) > 1);
+  }
+  if (k == 0) return out;
+  if (dup) {
+    // Two equal rows: c_i = c_j = 1 is a nonzero message with the zero
+    // codeword, so max_zeros = 49.
+    out.result = kN;
+    return out;
+  }
+  if (k == 1) {
+    // All nonzero multiples of one row have the row's zero set.
+    const int row = s_idx[0];
+    const int z0 = (lane < kN && M[row * kN + lane] == 0) ? 1 : 0;
+    const int z1 = (lane + 32 < kN && M[row * kN + lane + 32] == 0) ? 1 : 0;
+    out.result = __popc(__ballot_sync(0xffffffffu, z0)) + __popc(__ballot_sync(0xffffffffu, z1));
+    return out;
+  }
+  const int R = min(R_param, k);
+  const int H = k - R;
+  out.R = R;
+  out.H = H;
+  // Row order: leading head rows in general position (orbit mode).
+  if (lane == 0) {
+    int used = 0;  // bitmask over set positions
+    int nsel = 0;
+    if (enumeration == TG_ENUM_ORBIT) {
+      for (int pos = 0; pos < H; ++pos) {
+        int best = -1, best_cost = 1 << 30;
+        for (int cand = 0; cand < k; ++cand) {
+          if (used >> cand & 1) continue;
+          int cost = 0;
+          for (int x = 0; x < nsel; ++x)
+            for (int y = x + 1; y < nsel; ++y)
+              cost += collinear3(s_idx[s_row[x]], s_idx[s_row[y]], s_idx[cand]) ? 1 : 0;
+          if (cost < best_cost) { best_cost = cost; best = cand; }
+        }
+        s_row[nsel++] = best;
+        used |= 1 << best;
+      }
+    }
+    for (int cand = 0; cand < k; ++cand)
+      if (!(used >> cand & 1)) s_row[nsel++] = cand;
+  }
+  __syncwarp();
+
+  // Bit-sliced basis, coordinates j = lane and 32 + lane.
+  const int last = s_idx[s_row[k - 1]];
+  const bool hist = variant == TG_VARIANT_HISTOGRAM;
+  uint32_t inv_lo = 1, inv_hi = 1;
+  if (hist) {
+    inv_lo = c_inv[M[last * kN + lane]];
+    inv_hi = lane + 32 < kN ? c_inv[M[last * kN + lane + 32]] : 0u;
+  }
+  for (int r = 0; r < k; ++r) {
+    const int row = s_idx[s_row[r]];
+    const uint32_t g_lo = M[row * kN + lane];
+    const uint32_t g_hi = lane + 32 < kN ? M[row * kN + lane + 32] : 0u;
+    uint32_t e = 1;  // alpha^t
+    for (int t = 0; t < 3; ++t) {
+      uint32_t v_lo = c_mul[e * 8 + g_lo];
+      uint32_t v_hi = c_mul[e * 8 + g_hi];
+      if (hist) {
+        v_lo = c_mul[v_lo * 8 + inv_lo];
+        v_hi = lane + 32 < kN ? c_mul[v_hi * 8 + inv_hi] : 0u;
+      }
+      const V6 v = ballot_planes(lane, v_lo, v_hi);
+      if (lane == 0) v6_stg(B + r * 3 + t, v);
+      e = c_mul[e * 8 + 2];
+    }
+  }
+
+  // Message patterns over the head rows.
+  uint64_t n_tasks = 0;
+  int np = 0;
+  if (lane == 0) {
+    uint64_t acc = 0;
+    cum[np] = acc; info[np] = pat_pack(0, 0, 0, 0, 0, H); ++np; acc += 1;
+    if (enumeration == TG_ENUM_ORBIT) {
+      for (int i0 = 0; i0 < H; ++i0) {
+        cum[np] = acc; info[np] = pat_pack(i0, 0, 0, 1, 0, H); ++np; acc += 1;
+      }
+      for (int i0 = 0; i0 < H; ++i0)
+        for (int i1 = i0 + 1; i1 < H; ++i1) {
+          cum[np] = acc; info[np] = pat_pack(i0, i1, 0, 2, 0, H); ++np; acc += 1;
+        }
+      for (int i0 = 0; i0 < H; ++i0)
+        for (int i1 = i0 + 1; i1 < H; ++i1)
+          for (int i2 = i1 + 1; i2 < H; ++i2) {
+            const bool col = collinear3(s_idx[s_row[i0]], s_idx[s_row[i1]], s_idx[s_row[i2]]);
+            cum[np] = acc;
+            info[np] = pat_pack(i0, i1, i2, 3, col ? 1 : 0, i2 + 1);
+            ++np;
+            acc += (col ? 7ull : 1ull) * pow8(H - 1 - i2);
+          }
+    } else {
+      for (int i0 = 0; i0 < H; ++i0) {
+        cum[np] = acc; info[np] = pat_pack(i0, 0, 0, 1, 0, i0 + 1); ++np;
+        acc += pow8(H - 1 - i0);
+      }
+    }
+    n_tasks = acc;
+  }
+  out.n_tasks = __shfl_sync(0xffffffffu, n_tasks, 0);
+  out.n_pat = __shfl_sync(0xffffffffu, np, 0);
+  return out;
+}
+
 __global__ void __launch_bounds__(kPrepWarps * 32)
 prep_exact_kernel(DistArgs a) {
   __shared__ int s_idx[kPrepWarps][32];
@@ -165,7 +296,6 @@ prep_exact_kernel(DistArgs a) {
   d.set_id = c;
   d.tmax = kN - (a.target ? a.target[c] : a.td_default);
   d.flags = 0;
-  int result = 0;
   bool ok = true;
   if (klong < 0 || klong > a.k_max) {
     ok = false;
@@ -179,131 +309,27 @@ prep_exact_kernel(DistArgs a) {
     ok = false;
     if (lane == 0) report_status(a.hdr, TG_ERR_BAD_INPUT);
   }
-  bool dup = false;
-  if (ok && k > 1) {
-    const unsigned act = __ballot_sync(0xffffffffu, lane < k);
-    const unsigned m = __match_any_sync(0xffffffffu, lane < k ? my : -1 - lane);
-    dup = __any_sync(0xffffffffu, (act >> lane & 1u) && __popc(m) > 1);
-  }
   if (lane < 32) s_idx[w][lane] = my;
   __syncwarp();
-
-  uint64_t n_tasks = 0;
-  if (!ok || k == 0) {
-    result = 0;
-  } else if (dup) {
-    // Two equal rows: c_i = c_j = 1 is a nonzero message with the zero
-    // codeword, so max_zeros = 49.
-    result = kN;
-  } else if (k == 1) {
-    // All nonzero multiples of one row have the row's zero set.
-    const int row = s_idx[w][0];
-    const int z0 = (lane < kN && a.tab.M[row * kN + lane] == 0) ? 1 : 0;
-    const int z1 = (lane + 32 < kN && a.tab.M[row * kN + lane + 32] == 0) ? 1 : 0;
-    result = __popc(__ballot_sync(0xffffffffu, z0)) + __popc(__ballot_sync(0xffffffffu, z1));
-  } else {
-    const int R = min(a.R, k);
-    const int H = k - R;
-    d.R = R;
-    d.H = H;
-    // Row order: leading head rows in general position (orbit mode).
-    if (lane == 0) {
-      int used = 0;  // bitmask over set positions
-      int nsel = 0;
-      if (a.enumeration == TG_ENUM_ORBIT) {
-        for (int pos = 0; pos < H; ++pos) {
-          int best = -1, best_cost = 1 << 30;
-          for (int cand = 0; cand < k; ++cand) {
-            if (used >> cand & 1) continue;
-            int cost = 0;
-            for (int x = 0; x < nsel; ++x)
-              for (int y = x + 1; y < nsel; ++y)
-                cost += collinear3(s_idx[w][s_row[w][x]], s_idx[w][s_row[w][y]],
-                                   s_idx[w][cand]) ? 1 : 0;
-            if (cost < best_cost) { best_cost = cost; best = cand; }
-          }
-          s_row[w][nsel++] = best;
-          used |= 1 << best;
-        }
-      }
-      for (int cand = 0; cand < k; ++cand)
-        if (!(used >> cand & 1)) s_row[w][nsel++] = cand;
-    }
-    __syncwarp();
-
-    // Bit-sliced basis alpha^t * row_r (direct) or alpha^t * row_r / last row
-    // (histogram), coordinates j = lane and 32 + lane.
-    const int last = s_idx[w][s_row[w][k - 1]];
-    const bool hist = a.variant == TG_VARIANT_HISTOGRAM;
-    uint32_t inv_lo = 1, inv_hi = 1;
-    if (hist) {
-      inv_lo = c_inv[a.tab.M[last * kN + lane]];
-      inv_hi = lane + 32 < kN ? c_inv[a.tab.M[last * kN + lane + 32]] : 0u;
-    }
+  PrepResult pr{0, 0ull, 0, 0, 0};
+  if (ok) {
     V6* B = a.basis + size_t(c) * a.basis_stride;
-    for (int r = 0; r < k; ++r) {
-      const int row = s_idx[w][s_row[w][r]];
-      const uint32_t g_lo = a.tab.M[row * kN + lane];
-      const uint32_t g_hi = lane + 32 < kN ? a.tab.M[row * kN + lane + 32] : 0u;
-      uint32_t e = 1;  // alpha^t
-      for (int t = 0; t < 3; ++t) {
-        uint32_t v_lo = c_mul[e * 8 + g_lo];
-        uint32_t v_hi = c_mul[e * 8 + g_hi];
-        if (hist) {
-          v_lo = c_mul[v_lo * 8 + inv_lo];
-          v_hi = lane + 32 < kN ? c_mul[v_hi * 8 + inv_hi] : 0u;
-        }
-        const V6 v = ballot_planes(lane, v_lo, v_hi);
-        if (lane == 0) v6_stg(B + r * 3 + t, v);
-        e = c_mul[e * 8 + 2];
-      }
-    }
-
-    // Message patterns over the head rows.
-    if (lane == 0) {
-      uint64_t* cum = a.pat_cum + size_t(c) * a.pat_stride;
-      uint32_t* info = a.pat_info + size_t(c) * a.pat_stride;
-      int np = 0;
-      uint64_t acc = 0;
-      cum[np] = acc; info[np] = pat_pack(0, 0, 0, 0, 0, H); ++np; acc += 1;
-      if (a.enumeration == TG_ENUM_ORBIT) {
-        for (int i0 = 0; i0 < H; ++i0) {
-          cum[np] = acc; info[np] = pat_pack(i0, 0, 0, 1, 0, H); ++np; acc += 1;
-        }
-        for (int i0 = 0; i0 < H; ++i0)
-          for (int i1 = i0 + 1; i1 < H; ++i1) {
-            cum[np] = acc; info[np] = pat_pack(i0, i1, 0, 2, 0, H); ++np; acc += 1;
-          }
-        for (int i0 = 0; i0 < H; ++i0)
-          for (int i1 = i0 + 1; i1 < H; ++i1)
-            for (int i2 = i1 + 1; i2 < H; ++i2) {
-              const bool col = collinear3(s_idx[w][s_row[w][i0]], s_idx[w][s_row[w][i1]],
-                                          s_idx[w][s_row[w][i2]]);
-              cum[np] = acc;
-              info[np] = pat_pack(i0, i1, i2, 3, col ? 1 : 0, i2 + 1);
-              ++np;
-              acc += (col ? 7ull : 1ull) * pow8(H - 1 - i2);
-            }
-      } else {
-        for (int i0 = 0; i0 < H; ++i0) {
-          cum[np] = acc; info[np] = pat_pack(i0, 0, 0, 1, 0, i0 + 1); ++np;
-          acc += pow8(H - 1 - i0);
-        }
-      }
-      d.n_pat = np;
-      n_tasks = acc;
-    }
-    n_tasks = __shfl_sync(0xffffffffu, n_tasks, 0);
-    d.n_pat = __shfl_sync(0xffffffffu, d.n_pat, 0);
+    uint64_t* cum = a.pat_cum + size_t(c) * a.pat_stride;
+    uint32_t* info = a.pat_info + size_t(c) * a.pat_stride;
+    pr = prep_code(lane, k, s_idx[w], s_row[w], a.R, a.enumeration, a.variant, a.tab.M, B, cum,
+                   info);
   }
   if (lane == 0) {
     d.k = k;
-    d.n_tasks = n_tasks;
+    d.R = pr.R;
+    d.H = pr.H;
+    d.n_pat = pr.n_pat;
+    d.n_tasks = pr.n_tasks;
     a.desc[c] = d;
-    a.out[c] = result;
+    a.out[c] = pr.result;
     a.abort[c] = 0;
-    if (n_tasks) {
-      atomicAdd(&a.hdr->codewords, (unsigned long long)(n_tasks * pow8(d.R)));
+    if (pr.n_tasks) {
+      atomicAdd(&a.hdr->codewords, (unsigned long long)(pr.n_tasks * pow8(pr.R)));
     }
     if (ok && k > 0) atomicAdd(&a.hdr->ref_messages, double(pow8(k)) - 1.0);
   }
@@ -377,6 +403,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_tasks_kernel(DistArgs a) {
 
 // Start vector of local task q of a pattern: the head coefficients in the
 // domain of the basis.
+template <bool kCG = false>
 __device__ __forceinline__ V6 task_start(const V6* B, uint32_t info, uint64_t q, int H) {
   const int i0 = int(info & 31u), i1 = int((info >> 5) & 31u), i2 = int((info >> 10) & 31u);
   const int nfix = int((info >> 15) & 3u);
@@ -389,17 +416,17 @@ __device__ __forceinline__ V6 task_start(const V6* B, uint32_t info, uint64_t q,
     c2 = int(q % 7ull) + 1;
     q /= 7ull;
   }
-  if (nfix >= 1) v6_xor(s, v6_ldg(B + i0 * 3));
-  if (nfix >= 2) v6_xor(s, v6_ldg(B + i1 * 3));
+  if (nfix >= 1) v6_xor(s, v6_load<kCG>(B + i0 * 3));
+  if (nfix >= 2) v6_xor(s, v6_load<kCG>(B + i1 * 3));
   if (nfix >= 3) {
     for (int t = 0; t < 3; ++t)
-      if (c2 >> t & 1) v6_xor(s, v6_ldg(B + i2 * 3 + t));
+      if (c2 >> t & 1) v6_xor(s, v6_load<kCG>(B + i2 * 3 + t));
   }
   for (int r = H - 1; r >= ff; --r) {
     const int dgt = int(q & 7ull);
     q >>= 3;
     for (int t = 0; t < 3; ++t)
-      if (dgt >> t & 1) v6_xor(s, v6_ldg(B + r * 3 + t));
+      if (dgt >> t & 1) v6_xor(s, v6_load<kCG>(B + r * 3 + t));
   }
   return s;
 }
@@ -451,6 +478,52 @@ __device__ __forceinline__ bool claim_task(const DistArgs& a, uint64_t total, in
   return true;
 }
 
+// One task of the histogram walk: the Gray walk of the tail rows H..k-2 from
+// the pattern's start vector, 8 codewords per state.  Returns the largest
+// zero count seen; sets `aborted` when it exceeds tmax.  Polls *abort_flag
+// every 512 codewords and stops when another task aborted the code.
+template <bool kCG = false>
+__device__ __forceinline__ int hist_task(const V6* B, uint32_t info, uint64_t q, int H, int k,
+                                         int R, int tmax, const int32_t* abort_flag,
+                                         bool& aborted) {
+  V6 w = task_start<kCG>(B, info, q, H);
+  const bool zero_head = ((info >> 15) & 3u) == 0u;
+  const V6 g0 = v6_load<kCG>(B + (k - 2) * 3 + 0);
+  const V6 g1 = v6_load<kCG>(B + (k - 2) * 3 + 1);
+  const V6 g2 = v6_load<kCG>(B + (k - 2) * 3 + 2);
+  const uint32_t n_mid = 1u << (3 * (R - 2));
+  int m = 0;
+  aborted = false;
+  for (uint32_t mi = 0; mi < n_mid; ++mi) {
+    if (mi) {
+      const int f = __ffs(int(mi)) - 1;
+      const int row = k - 3 - f / 3;
+      v6_xor(w, v6_load<kCG>(B + row * 3 + f % 3));
+    }
+    hist8(w, m, mi != 0u || !zero_head);
+    v6_xor(w, g0); hist8(w, m, true);
+    v6_xor(w, g1); hist8(w, m, true);
+    v6_xor(w, g0); hist8(w, m, true);
+    v6_xor(w, g2); hist8(w, m, true);
+    v6_xor(w, g0); hist8(w, m, true);
+    v6_xor(w, g1); hist8(w, m, true);
+    v6_xor(w, g0); hist8(w, m, true);
+    if (m > tmax) {
+      aborted = true;
+      break;
+    }
+    if ((mi & 7u) == 7u && ld_flag(abort_flag)) break;
+  }
+  return m;
+}
+
+// Moves the task counter past the remaining tasks of an aborted code: every
+// task in [counter, task_off[c + 1]) belongs to code c once a lane of c has
+// been claimed, so the jump loses no other code's work.
+__device__ __forceinline__ void skip_code(const DistArgs& a, int c) {
+  atomicMax(&a.hdr->counter, static_cast<unsigned long long>(__ldg(a.task_off + c + 1)));
+}
+
 template <int kTPB, int kMinBlocks>
 __global__ void __launch_bounds__(kTPB, kMinBlocks) walk_hist_kernel(DistArgs a) {
   const int lane = threadIdx.x & 31;
@@ -460,7 +533,11 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) walk_hist_kernel(DistArgs a)
     int c;
     bool active;
     if (!claim_task(a, total, lane, t, c, active)) break;
-    if (!active || ld_flag(a.abort + c)) continue;
+    if (!active) continue;
+    if (ld_flag(a.abort + c)) {
+      skip_code(a, c);
+      continue;
+    }
     const CodeDesc d = a.desc[c];
     const uint64_t local = t - __ldg(a.task_off + c);
     const uint64_t* cum = a.pat_cum + size_t(c) * a.pat_stride;
@@ -468,39 +545,13 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) walk_hist_kernel(DistArgs a)
     const uint64_t q = local - __ldg(cum + p);
     const uint32_t info = __ldg(a.pat_info + size_t(c) * a.pat_stride + p);
     const V6* B = a.basis + size_t(c) * a.basis_stride;
-    V6 w = task_start(B, info, q, d.H);
-    const bool zero_head = ((info >> 15) & 3u) == 0u;
-    const int k = d.k;
-    const V6 g0 = v6_ldg(B + (k - 2) * 3 + 0);
-    const V6 g1 = v6_ldg(B + (k - 2) * 3 + 1);
-    const V6 g2 = v6_ldg(B + (k - 2) * 3 + 2);
-    const int n_mid_bits = 3 * (d.R - 2);
-    const uint32_t n_mid = 1u << n_mid_bits;
-    const int tmax = d.tmax;
-    int m = 0;
     bool aborted = false;
-    for (uint32_t mi = 0; mi < n_mid; ++mi) {
-      if (mi) {
-        const int f = __ffs(int(mi)) - 1;
-        const int row = k - 3 - f / 3;
-        v6_xor(w, v6_ldg(B + row * 3 + f % 3));
-      }
-      hist8(w, m, mi != 0u || !zero_head);
-      v6_xor(w, g0); hist8(w, m, true);
-      v6_xor(w, g1); hist8(w, m, true);
-      v6_xor(w, g0); hist8(w, m, true);
-      v6_xor(w, g2); hist8(w, m, true);
-      v6_xor(w, g0); hist8(w, m, true);
-      v6_xor(w, g1); hist8(w, m, true);
-      v6_xor(w, g0); hist8(w, m, true);
-      if (m > tmax) {
-        aborted = true;
-        break;
-      }
-      if ((mi & 63u) == 63u && ld_flag(a.abort + c)) break;
-    }
+    const int m = hist_task(B, info, q, d.H, d.k, d.R, d.tmax, a.abort + c, aborted);
     if (m > 0) atomicMax(a.out + c, m);
-    if (aborted) atomicExch(a.abort + c, 1);
+    if (aborted) {
+      atomicExch(a.abort + c, 1);
+      skip_code(a, c);
+    }
   }
 }
 
@@ -513,7 +564,11 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) walk_direct_kernel(DistArgs 
     int c;
     bool active;
     if (!claim_task(a, total, lane, t, c, active)) break;
-    if (!active || ld_flag(a.abort + c)) continue;
+    if (!active) continue;
+    if (ld_flag(a.abort + c)) {
+      skip_code(a, c);
+      continue;
+    }
     const CodeDesc d = a.desc[c];
     const uint64_t local = t - __ldg(a.task_off + c);
     const uint64_t* cum = a.pat_cum + size_t(c) * a.pat_stride;
@@ -565,7 +620,10 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) walk_direct_kernel(DistArgs 
     }
     const int m = kN - wmin;
     if (m > 0) atomicMax(a.out + c, m);
-    if (aborted) atomicExch(a.abort + c, 1);
+    if (aborted) {
+      atomicExch(a.abort + c, 1);
+      skip_code(a, c);
+    }
   }
 }
 
@@ -636,7 +694,11 @@ __global__ void __launch_bounds__(kTPB) walk_sampled_kernel(DistArgs a) {
     int c;
     bool active;
     if (!claim_task(a, total, lane, t, c, active)) break;
-    if (!active || ld_flag(a.abort + c)) continue;
+    if (!active) continue;
+    if (ld_flag(a.abort + c)) {
+      skip_code(a, c);
+      continue;
+    }
     const CodeDesc d = a.desc[c];
     const uint64_t j = t - __ldg(a.task_off + c);
     const V6* T = a.bitpat + size_t(c) * a.bitpat_stride;
@@ -678,7 +740,10 @@ __global__ void __launch_bounds__(kTPB) walk_sampled_kernel(DistArgs a) {
       if ((wid & 15ull) == 0ull && ld_flag(a.abort + c)) break;
     }
     if (m > 0) atomicMax(a.out + c, m);
-    if (aborted) atomicExch(a.abort + c, 1);
+    if (aborted) {
+      atomicExch(a.abort + c, 1);
+      skip_code(a, c);
+    }
   }
 }
 
@@ -737,3 +802,5 @@ int run_walk(const DistArgs& args, int sm_count, int blocks_per_sm, int tpb, cud
 }
 
 }  // namespace tg
+
+#include "serve_kernel.cuh"

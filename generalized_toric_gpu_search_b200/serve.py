@@ -1,0 +1,219 @@
+"""Served search stream: max_zeros requests evaluated as they arrive.
+
+`ToricServer` is the client side of the device-resident request loop
+(tg_server_* in include/toric_b200.h).  A search driver -- the BFS expansion
+of champion_search_canonical.py:496-512 or the generations of
+evolve_search.py:398-420 -- submits candidate sets one by one with the
+threshold it currently holds (its best-known distance for that k) and gets a
+future per request.
+
+What the loop does per request, on the GPU:
+  * admission: requests take one of a fixed pool of device slots, sized from
+    free device memory; when all are busy they wait here, on the host, and
+    enter as answers free slots;
+  * canonical dedup: the AGL2(F7) canonical mask keys a device hash table; a
+    request whose equivalent was already answered is answered from it when
+    that answer decides this request's threshold (an exact earlier value, or
+    an earlier failure whose witness exceeds this threshold); a request whose
+    equivalent is still running waits for it;
+  * evaluation: the tasks of every admitted request share one persistent
+    grid, oldest request first, so requests that arrive while others run
+    overlap with them on the device (continuous batching).
+Answers follow the batch oracle's contract: `passed` (max_zeros <= 49 - td,
+value exact) or a failure witness above 49 - td.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import threading
+import time
+from collections import deque
+from concurrent.futures import Future
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib
+from .distance import ToricContext
+from .tables import N_POINTS, build_eval_matrix
+
+
+@dataclass(frozen=True)
+class ServeAnswer:
+    """Answer of one served request."""
+
+    id: int
+    max_zeros: int
+    passed: bool           # max_zeros <= 49 - target_distance (value exact)
+    dedup: bool            # answered from an equivalent earlier request
+    latency_s: float       # submit -> answer seen by the host
+    device_s: float        # loop took the request -> answer written (device clock)
+
+    @property
+    def min_distance(self) -> int:
+        return N_POINTS - self.max_zeros
+
+
+class ToricServer:
+    """Client of the device-resident max_zeros request loop on one GPU."""
+
+    def __init__(self, device_id: int = 0, M: np.ndarray | None = None, *, k_max: int = 15,
+                 max_slots: int = 0, memory_fraction: float = 0.25, tail_rows: int = 0,
+                 table_capacity: int = 0, idle_us: int = 0, life_ms: int = 0,
+                 blocks_per_sm: int = 0):
+        self.ctx = ToricContext(device_id, build_eval_matrix() if M is None else M)
+        self.device = torch.device("cuda", device_id)
+        lib = _lib.load()
+        self._lib = lib
+        self.params = _lib.ServerParams(
+            max_slots=max_slots, k_max=k_max, tail_rows=tail_rows, blocks_per_sm=blocks_per_sm,
+            idle_us=idle_us, life_ms=life_ms, table_capacity=table_capacity,
+            memory_fraction=memory_fraction)
+        slots, dev_b, host_b = ctypes.c_int32(0), ctypes.c_size_t(0), ctypes.c_size_t(0)
+        _lib.check(lib.tg_server_layout(self.ctx.handle, ctypes.byref(self.params),
+                                        ctypes.byref(slots), ctypes.byref(dev_b),
+                                        ctypes.byref(host_b)), "tg_server_layout")
+        self.slots = int(slots.value)
+        self.params.max_slots = self.slots  # pin the admitted pool size
+        self._arena = torch.empty(int(dev_b.value), dtype=torch.uint8, device=self.device)
+        self._host = torch.empty(int(host_b.value), dtype=torch.uint8, pin_memory=True)
+        handle = ctypes.c_void_p()
+        _lib.check(lib.tg_server_create(self.ctx.handle, ctypes.byref(self.params),
+                                        self._arena.data_ptr(), self._arena.numel(),
+                                        self._host.data_ptr(), self._host.numel(),
+                                        ctypes.byref(handle)), "tg_server_create")
+        self.handle = handle
+        self.k_max = k_max
+        self._pending: deque = deque()
+        self._inflight: dict[int, tuple[Future, float]] = {}
+        self._cv = threading.Condition()
+        self._closed = False
+        self._error: BaseException | None = None
+        self._results = (_lib.ServerResult * 512)()
+        self._thread = threading.Thread(target=self._pump_loop, name="toric-server", daemon=True)
+        self._thread.start()
+
+    # -- client API -----------------------------------------------------------
+
+    def submit(self, indices, target_distance: int) -> Future:
+        """Queues one request; the future yields a ServeAnswer."""
+        idx = np.ascontiguousarray(np.asarray(indices, dtype=np.int32).reshape(-1))
+        if idx.size > self.k_max:
+            raise ValueError(f"request has k = {idx.size} > k_max = {self.k_max}")
+        if idx.size and (int(idx.min()) < 0 or int(idx.max()) >= N_POINTS):
+            raise ValueError("exponent indices must lie in 0..48")
+        fut: Future = Future()
+        with self._cv:
+            if self._closed:
+                raise RuntimeError("server is closed")
+            if self._error is not None:
+                raise RuntimeError("server failed") from self._error
+            self._pending.append((idx, int(target_distance), fut, time.perf_counter()))
+            self._cv.notify()
+        return fut
+
+    def evaluate(self, requests, timeout: float = 600.0) -> list[ServeAnswer]:
+        """Submits (indices, target_distance) pairs and waits for all answers."""
+        futs = [self.submit(s, td) for s, td in requests]
+        return [f.result(timeout=timeout) for f in futs]
+
+    def stats(self) -> dict:
+        c = (ctypes.c_uint64 * 8)()
+        _lib.check(self._lib.tg_server_stats(self.handle, c), "tg_server_stats")
+        keys = ["published", "finished", "outstanding", "loop_launches", "tasks",
+                "codewords", "dedup_answers", "device_status"]
+        return dict(zip(keys, (int(x) for x in c)))
+
+    def close(self) -> None:
+        with self._cv:
+            if self._closed:
+                return
+            self._closed = True
+            self._cv.notify()
+        self._thread.join(timeout=30)
+        if self.handle:
+            _lib.check(self._lib.tg_server_destroy(self.handle), "tg_server_destroy")
+            self.handle = ctypes.c_void_p()
+        self.ctx.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- pump thread ----------------------------------------------------------
+
+    def _admit(self) -> int:
+        """Moves waiting requests into free device slots."""
+        lib = self._lib
+        admitted = 0
+        rid = ctypes.c_uint32(0)
+        while True:
+            with self._cv:
+                if not self._pending:
+                    return admitted
+                idx, td, fut, t0 = self._pending[0]
+            st = lib.tg_server_submit(self.handle, idx.ctypes.data if idx.size else None,
+                                      idx.size, td, ctypes.byref(rid))
+            if st == _lib.TG_ERR_CAPACITY:
+                return admitted
+            with self._cv:
+                self._pending.popleft()
+            if st != _lib.TG_OK:
+                try:
+                    _lib.check(st, "tg_server_submit")
+                except BaseException as exc:  # noqa: BLE001 - delivered to the caller
+                    fut.set_exception(exc)
+                continue
+            self._inflight[int(rid.value)] = (fut, t0)
+            admitted += 1
+
+    def _collect(self) -> int:
+        lib = self._lib
+        n = ctypes.c_int32(0)
+        _lib.check(lib.tg_server_poll(self.handle, self._results, len(self._results),
+                                      ctypes.byref(n)), "tg_server_poll")
+        now = time.perf_counter()
+        for i in range(n.value):
+            r = self._results[i]
+            fut, t0 = self._inflight.pop(int(r.id))
+            flags = int(r.flags)
+            if flags & _lib.TG_RESULT_BAD_INPUT:
+                fut.set_exception(ValueError("request rejected by the device (bad input)"))
+                continue
+            fut.set_result(ServeAnswer(
+                id=int(r.id), max_zeros=int(r.max_zeros),
+                passed=bool(flags & _lib.TG_RESULT_PASS),
+                dedup=bool(flags & _lib.TG_RESULT_DEDUP), latency_s=now - t0,
+                device_s=(int(r.t_done_ns) - int(r.t_admit_ns)) / 1e9))
+        return n.value
+
+    def _pump_loop(self) -> None:
+        running = ctypes.c_int32(0)
+        try:
+            while True:
+                with self._cv:
+                    if self._closed:
+                        break
+                    if not self._pending and not self._inflight:
+                        self._cv.wait(timeout=0.05)
+                        continue
+                busy = self._admit()
+                _lib.check(self._lib.tg_server_pump(self.handle, ctypes.byref(running)),
+                           "tg_server_pump")
+                busy += self._collect()
+                if not busy:
+                    time.sleep(5e-5)
+        except BaseException as exc:  # noqa: BLE001 - surfaced to every waiter
+            with self._cv:
+                self._error = exc
+                waiters = [f for f, _ in self._inflight.values()]
+                waiters += [p[2] for p in self._pending]
+                self._inflight.clear()
+                self._pending.clear()
+            for f in waiters:
+                if not f.done():
+                    f.set_exception(exc)

@@ -218,6 +218,66 @@ int tg_hashset_insert(void* d_table, int64_t capacity, const uint64_t* d_keys,
                       int32_t n, uint32_t call_id, uint8_t* d_is_new,
                       int32_t* d_n_new, int32_t* d_status, void* stream);
 
+/* ---- served search stream (device-resident request loop) ---------------- */
+
+/* A server evaluates max_zeros requests as they arrive: requests are admitted
+ * into a fixed pool of device slots (sized from free device memory), each is
+ * deduplicated by its AGL2(F7) canonical form in a device hash table, carries
+ * its own early-exit threshold, and has its tasks interleaved with those of
+ * the requests already on the GPU by one persistent loop kernel.  This is the
+ * B200 form of the reference's host pipeline _pipelined_eval + _dispatch
+ * (champion_search_canonical.py:281-378, 237-271) and evolve_search's
+ * evaluate_sets (evolve_search.py:266-282), request by request. */
+
+typedef struct tg_server tg_server;
+
+typedef struct tg_server_params {
+  int32_t max_slots;       /* request slots; 0 = from free device memory     */
+  int32_t k_max;           /* largest request size, <= 21                    */
+  int32_t tail_rows;       /* R of the task walk; 0 = 4                      */
+  int32_t blocks_per_sm;   /* loop CTAs (128 threads) per SM; 0 = 8          */
+  int32_t idle_us;         /* the loop exits after this long without work; 0 = 2000 */
+  int32_t life_ms;         /* one loop launch ends after this long; 0 = 250  */
+  int64_t table_capacity;  /* dedup table slots, power of two; 0 = 2^20; -1 = no dedup */
+  double memory_fraction;  /* share of free device memory for slots (max_slots == 0); 0 = 0.25 */
+} tg_server_params;
+
+#define TG_RESULT_PASS 1      /* max_zeros <= 49 - td; the value is exact          */
+#define TG_RESULT_FAIL 2      /* a codeword beyond the threshold; value is a witness */
+#define TG_RESULT_DEDUP 4     /* answered from an earlier request of the same canonical form */
+#define TG_RESULT_BAD_INPUT 8 /* k or an index out of range                         */
+
+typedef struct tg_server_result {
+  uint32_t id;          /* the id tg_server_submit returned                  */
+  int32_t max_zeros;
+  int32_t flags;        /* TG_RESULT_* bits                                  */
+  int32_t pad;
+  uint64_t t_admit_ns;  /* device globaltimer when the loop took the request */
+  uint64_t t_done_ns;   /* device globaltimer when the answer was written    */
+} tg_server_result;
+
+/* Slots, device bytes and page-locked host bytes a server needs. */
+int tg_server_layout(tg_context* ctx, const tg_server_params* p, int32_t* h_slots,
+                     size_t* h_device_bytes, size_t* h_host_bytes);
+/* Creates a server in caller memory: d_arena (device, 256-byte aligned) and
+ * h_pinned (page-locked host memory the device can map, e.g. cudaHostAlloc). */
+int tg_server_create(tg_context* ctx, const tg_server_params* p, void* d_arena,
+                     size_t device_bytes, void* h_pinned, size_t host_bytes,
+                     tg_server** out);
+/* Queues one request; TG_ERR_CAPACITY when every slot is busy. */
+int tg_server_submit(tg_server* srv, const int32_t* h_indices, int32_t k,
+                     int32_t target_distance, uint32_t* h_id);
+/* (Re)launches the loop kernel when requests are outstanding and it has
+ * exited; *h_running = 1 while a loop launch is executing. */
+int tg_server_pump(tg_server* srv, int32_t* h_running);
+/* Collects up to max finished results (in completion order) and frees slots. */
+int tg_server_poll(tg_server* srv, tg_server_result* h_out, int32_t max, int32_t* h_n);
+/* Counters: [0] published, [1] finished, [2] outstanding, [3] loop launches,
+ * [4] tasks run, [5] codewords planned, [6] dedup answers, [7] device status. */
+int tg_server_stats(tg_server* srv, uint64_t* h_counters8);
+/* Stops the loop (bounded wait) and frees the server object. */
+int tg_server_destroy(tg_server* srv);
+
 /* ---- integer pipe throughput (roofline denominators) --------------------- */
 
 /* Measures per-SM issue rates (operations per SM per clock) of the integer
