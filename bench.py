@@ -250,6 +250,161 @@ def run_reference_arm(args, d: Dist) -> None:
 
 
 # ---------------------------------------------------------------------------
+# Secondary configurations (rank 0, reported beside the headline)
+# ---------------------------------------------------------------------------
+
+# Best-known minimum distances of [49, k] codes over GF(8) bundled with the
+# reference's evolutionary notebook (used when codetables.de is unreachable).
+FALLBACK_BEST_D = {12: 28, 13: 27, 14: 26, 15: 24, 16: 24, 17: 23, 18: 21, 19: 21}
+
+
+def random_masks(n: int, k_lo: int, k_hi: int, seed: int) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    keys = rng.random((n, 49))
+    ks = rng.integers(k_lo, k_hi + 1, size=n)
+    order = np.argsort(keys, axis=1)
+    sel = np.arange(49)[None, :] < ks[:, None]
+    bits = np.zeros((n, 49), dtype=bool)
+    np.put_along_axis(bits, order, sel, axis=1)
+    return (bits.astype(np.uint64) << np.arange(49, dtype=np.uint64)).sum(axis=1, dtype=np.uint64)
+
+
+def bench_canonical(dev: int, n: int = 1_000_000) -> dict:
+    """Canonical forms of n seeded 49-bit sets (popcount U{5..30}) and device
+    dedup of the canonical masks."""
+    import torch
+
+    from generalized_toric_gpu_search_b200 import _lib
+    from generalized_toric_gpu_search_b200.canonical import CanonicalDedup, CanonicalOracle
+
+    masks = random_masks(n, 5, 30, BASE_SEED + 3)
+    co = CanonicalOracle(dev)
+    d_in = torch.from_numpy(masks.view(np.int64)).to(f"cuda:{dev}")
+    out = torch.empty(n, dtype=torch.int64, device=f"cuda:{dev}")
+    s = torch.cuda.current_stream(dev)
+    lib = _lib.load()
+
+    def run():
+        _lib.check(lib.tg_canonical_masks(co.ctx.handle, d_in.data_ptr(), n, out.data_ptr(),
+                                          None, None, s.cuda_stream), "tg_canonical_masks")
+
+    run()
+    torch.cuda.synchronize()
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    dd = CanonicalDedup(dev, capacity=1 << 22)
+    e[0].record(s)
+    run()
+    e[1].record(s)
+    e[2].record(s)
+    _, n_new, _ = dd.insert_device(out, stream=s)
+    e[3].record(s)
+    torch.cuda.synchronize()
+    t_canon = e[0].elapsed_time(e[1]) / 1e3
+    t_dedup = e[2].elapsed_time(e[3]) / 1e3
+    return {"workload": f"{n:,} seeded 49-bit sets, popcount U{{5..30}}",
+            "canonical_sets_per_s": n / t_canon, "canonical_ms": 1e3 * t_canon,
+            "dedup_ms": 1e3 * t_dedup, "unique": int(n_new.item())}
+
+
+def bench_early_exit(dev: int, n: int = 2000) -> dict:
+    """n seeded sets of k = 15 against the k = 15 best-known distance."""
+    from generalized_toric_gpu_search_b200.distance import DistanceOracleCUDABP
+    from generalized_toric_gpu_search_b200.tables import build_eval_matrix
+
+    rng = np.random.default_rng(BASE_SEED + 5)
+    sets = [sorted(rng.choice(49, 15, replace=False).tolist()) for _ in range(n)]
+    td = FALLBACK_BEST_D[15]
+    o = DistanceOracleCUDABP(dev, build_eval_matrix())
+    o.max_zeros_batch(sets[:8], td)
+    t0 = time.perf_counter()
+    res = o.max_zeros_batch(sets, td)
+    dt = time.perf_counter() - t0
+    passed = sum(1 for r in res if r <= 49 - td)
+    return {"workload": f"{n} seeded sets, k=15, target_distance={td}",
+            "seconds": dt, "codes_per_s": n / dt, "passed": passed,
+            "reference_equivalent_messages_if_exhaustive": float(n * (8 ** 15 - 1))}
+
+
+def mutation_stream(n: int, seed: int, k_lo: int = 10, k_hi: int = 15):
+    """n requests: single-point mutations (add / remove / move one exponent)
+    of 256 seeded parents with |P| in k_lo..k_hi."""
+    rng = np.random.default_rng(seed)
+    parents = [sorted(rng.choice(49, int(rng.integers(k_lo, k_hi + 1)), replace=False).tolist())
+               for _ in range(256)]
+    out = []
+    for _ in range(n):
+        p = list(parents[int(rng.integers(len(parents)))])
+        free = [x for x in range(49) if x not in p]
+        op = int(rng.integers(3))
+        if op == 0 and len(p) < k_hi:
+            p.append(int(rng.choice(free)))
+        elif op == 1 and len(p) > k_lo:
+            p.pop(int(rng.integers(len(p))))
+        else:
+            p[int(rng.integers(len(p)))] = int(rng.choice(free))
+        out.append(sorted(p))
+    return out
+
+
+def bench_served(dev: int, n: int = 3000, rate: float = 300.0) -> dict:
+    """Served search stream: Poisson arrivals at `rate` per second of mutated
+    candidates, each with the running best-known d of its k as threshold."""
+    from generalized_toric_gpu_search_b200.serve import ToricServer
+
+    stream = mutation_stream(n, BASE_SEED + 7)
+    rng = np.random.default_rng(BASE_SEED + 11)
+    gaps = rng.exponential(1.0 / rate, size=n)
+    best = {k: FALLBACK_BEST_D.get(k, 1) for k in range(10, 16)}
+    import threading
+
+    lock = threading.Lock()
+
+    def on_done(fut, k):
+        a = fut.result()
+        if a.passed:
+            with lock:
+                if a.min_distance > best[k]:
+                    best[k] = a.min_distance
+
+    with ToricServer(dev, k_max=15) as srv:
+        srv.evaluate([(s, best[len(s)]) for s in stream[:32]])  # warm the loop
+        futs = []
+        t0 = time.perf_counter()
+        t_next = t0
+        for s, gap in zip(stream, gaps):
+            t_next += gap
+            while time.perf_counter() < t_next:
+                pass
+            with lock:
+                td = best[len(s)]
+            f = srv.submit(s, td)
+            f.add_done_callback(lambda fut, k=len(s): on_done(fut, k))
+            futs.append(f)
+        answers = [f.result(timeout=600) for f in futs]
+        total = time.perf_counter() - t0
+        st = srv.stats()
+        slots = srv.slots
+        # Saturation: a second stream of the same size submitted at once.
+        burst = mutation_stream(n, BASE_SEED + 13)
+        tb = time.perf_counter()
+        srv.evaluate([(s, best[len(s)]) for s in burst], timeout=600)
+        burst_s = time.perf_counter() - tb
+    lat = np.array([a.latency_s for a in answers])
+    dev_t = np.array([a.device_s for a in answers])
+    return {"workload": (f"{n:,} Poisson arrivals at {rate:.0f}/s, single mutations of 256 seeded "
+                         "parents, |P| 10..15, td = running best-known d per k"),
+            "codes_per_s": n / total, "seconds": total,
+            "p50_ms": 1e3 * float(np.percentile(lat, 50)),
+            "p99_ms": 1e3 * float(np.percentile(lat, 99)),
+            "device_p50_ms": 1e3 * float(np.percentile(dev_t, 50)),
+            "device_p99_ms": 1e3 * float(np.percentile(dev_t, 99)),
+            "dedup_answers": st["dedup_answers"], "passed": int(sum(a.passed for a in answers)),
+            "slots": slots, "loop_launches": st["loop_launches"],
+            "burst_codes_per_s": n / burst_s,
+            "best_known_d_end": best}
+
+
+# ---------------------------------------------------------------------------
 # B200 arm
 # ---------------------------------------------------------------------------
 
@@ -400,6 +555,12 @@ def run_b200_arm(args, d: Dist) -> None:
     achieved = POPC_PER_CODEWORD * codewords / walk_s
     peak = pipes.get("popc_per_clk_sm", 16.0) * sm_count * (mhz or 1965.0) * 1e6
 
+    extra = {}
+    if d.rank == 0 and not args.skip_extra:
+        extra["canonical_forms"] = bench_canonical(dev)
+        extra["early_exit_k15"] = bench_early_exit(dev)
+        extra["served_stream"] = bench_served(dev)
+
     cpu = None
     if d.rank == 0 and d.world == 1 and not args.skip_cpu:
         cpu = cpu_reference_rate(sets, 1 << 26, per_k=4)
@@ -436,6 +597,7 @@ def run_b200_arm(args, d: Dist) -> None:
             "plain_form": plain,
             "batched_vs_plain": (value / plain["value"]) if plain else None,
             "cpu_baseline": cpu,
+            **extra,
         }
         print(json.dumps(line), flush=True)
     del g_prep, g_walk
@@ -452,6 +614,8 @@ def main(argv=None) -> None:
     ap.add_argument("--blocks-per-sm", type=int, default=0)
     ap.add_argument("--skip-plain", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-extra", action="store_true",
+                    help="skip the canonical, early-exit and served-stream sections")
     ap.add_argument("--n-sets", type=int, default=N_SETS, help="sets per GPU (small cases)")
     ap.add_argument("--kmin", type=int, default=K_LO)
     ap.add_argument("--kmax", type=int, default=K_HI)

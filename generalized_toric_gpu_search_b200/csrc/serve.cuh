@@ -57,8 +57,12 @@ struct SrvDevHeader {
   unsigned long long dedup_hits;
   unsigned long long finished;
   unsigned int trace_n;                 // lo advances recorded so far
-  unsigned int pad;
+  unsigned int pub_mirror;              // device copy of SrvCtl::published
   unsigned long long trace[32][4];      // last lo advances: i|reason, id|state, n_tasks, claim
+  unsigned int stop_mirror;             // device copy of SrvCtl::stop
+  unsigned int pad1;
+  unsigned long long scan_steps;        // request entries looked at by scanners
+  unsigned long long host_reads;        // refreshes of the mirrors from host memory
 };
 
 struct SrvSlotHdr {
@@ -85,6 +89,7 @@ struct SrvArgs {
   uint8_t* slots;
   size_t slot_bytes;
   size_t basis_off, cum_off, info_off;
+  unsigned long long* ring;   // device copy of pubq, written by each request's preparer
   unsigned long long* keys;
   unsigned long long* vals;
   unsigned long long table_cap;

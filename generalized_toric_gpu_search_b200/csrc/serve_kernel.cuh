@@ -211,6 +211,7 @@ __device__ void srv_prepare(const SrvArgs& a, int lane, unsigned int req, int* s
   SrvSlotHdr* h = srv_slot(a, slot);
   const SrvInput* in = a.inputs + slot;
   if (lane == 0) {
+    *reinterpret_cast<volatile unsigned long long*>(a.ring + (req % unsigned(a.Q))) = e;
     *reinterpret_cast<volatile unsigned int*>(&h->state) = kSlotPrep;
     __threadfence();
     *reinterpret_cast<volatile unsigned int*>(&h->id) = req;
@@ -349,16 +350,26 @@ __global__ void __launch_bounds__(kSrvTPB, 8) serve_kernel(SrvArgs a) {
     atomicMax(&a.dh->last_activity, t_start);
     atomicAdd(&a.dh->launches, 1u);
   }
+  unsigned int iter = 0u;
+  bool was_idle = true;
   for (;;) {
     int action = 0;  // -1 exit, 0 idle, 1 prepare, 2 run, 3 resolve
     unsigned int arg = 0u, slot = 0u;
     unsigned long long c0 = 0ull;
     if (lane == 0) {
+      // Host memory is read over the bus: only an idle warp, or every warp
+      // once in 64 steps, refreshes the device mirrors of the host's counters.
+      if (was_idle || (++iter & 63u) == 0u) {
+        atomicMax(&a.dh->pub_mirror, ld_acquire_sys(&a.ctl->published));
+        if (ld_acquire_sys(&a.ctl->stop)) atomicExch(&a.dh->stop_mirror, 1u);
+        atomicAdd(&a.dh->host_reads, 1ull);
+      }
       const unsigned long long now = gtimer();
-      if (ld_acquire_sys(&a.ctl->stop) || now - t_start > a.life_ns) {
+      unsigned int steps = 0u;
+      if (ld_vol32(&a.dh->stop_mirror) || now - t_start > a.life_ns) {
         action = -1;
       } else {
-        const unsigned int pub = ld_acquire_sys(&a.ctl->published);
+        const unsigned int pub = ld_vol32(&a.dh->pub_mirror);
         unsigned int p = ld_vol32(&a.dh->prep_next);
         while (p < pub) {
           const unsigned int prev = atomicCAS(&a.dh->prep_next, p, p + 1u);
@@ -371,8 +382,10 @@ __global__ void __launch_bounds__(kSrvTPB, 8) serve_kernel(SrvArgs a) {
         }
         if (action == 0) {
           unsigned int lo = ld_vol32(&a.dh->lo);
-          for (unsigned int i = lo, n = 0; i < pub && n < unsigned(a.S) + 1u; ++i, ++n) {
-            const unsigned long long e = ld_sys64(a.pubq + (i % unsigned(a.Q)));
+          const unsigned int prepped = min(pub, ld_vol32(&a.dh->prep_next));
+          for (unsigned int i = lo, n = 0; i < prepped && n < unsigned(a.S) + 1u; ++i, ++n) {
+            ++steps;
+            const unsigned long long e = ld_vol64(a.ring + (i % unsigned(a.Q)));
             const unsigned int eg = static_cast<unsigned int>(e >> 32);
             bool finished = false;  // nothing left to claim or resolve at i
             unsigned int why = 0u, t_hid = 0u, t_st = 0u;
@@ -441,6 +454,7 @@ __global__ void __launch_bounds__(kSrvTPB, 8) serve_kernel(SrvArgs a) {
             }
           }
         }
+        if (steps) atomicAdd(&a.dh->scan_steps, static_cast<unsigned long long>(steps));
         if (action == 0) {
           const unsigned long long act = max(ld_vol64(&a.dh->last_activity), t_start);
           if (now > act + a.idle_ns) action = -1;
@@ -449,6 +463,7 @@ __global__ void __launch_bounds__(kSrvTPB, 8) serve_kernel(SrvArgs a) {
     }
     action = __shfl_sync(0xffffffffu, action, 0);
     if (action < 0) break;
+    was_idle = action == 0;
     if (action == 0) {
       __nanosleep(20000);
       continue;

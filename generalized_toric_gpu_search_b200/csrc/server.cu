@@ -22,7 +22,7 @@ static size_t a256(size_t x) { return (x + 255) & ~size_t(255); }
 struct SrvLayout {
   int S, Q, R, k_max, P;
   size_t slot_bytes, basis_off, cum_off, info_off;
-  size_t d_hdr, d_slots, d_keys, d_vals, d_total;
+  size_t d_hdr, d_slots, d_ring, d_keys, d_vals, d_total;
   size_t h_ctl, h_pubq, h_inputs, h_results, h_total;
   unsigned long long table_cap;
 };
@@ -83,6 +83,7 @@ static SrvLayout srv_layout(const tg_server_params& q, int S) {
   size_t off = 0;
   L.d_hdr = off;   off = a256(off + sizeof(SrvDevHeader));
   L.d_slots = off; off = a256(off + size_t(S) * L.slot_bytes);
+  L.d_ring = off;  off = a256(off + size_t(L.Q) * 8);
   L.d_keys = off;  off = a256(off + L.table_cap * 8);
   L.d_vals = off;  off = a256(off + L.table_cap * 8);
   L.d_total = off;
@@ -248,6 +249,7 @@ int tg_server_create(tg_context* ctx, const tg_server_params* p, void* d_arena,
   a.basis_off = L.basis_off;
   a.cum_off = L.cum_off;
   a.info_off = L.info_off;
+  a.ring = reinterpret_cast<unsigned long long*>(srv->d_arena + L.d_ring);
   a.keys = reinterpret_cast<unsigned long long*>(srv->d_arena + L.d_keys);
   a.vals = reinterpret_cast<unsigned long long*>(srv->d_arena + L.d_vals);
   a.table_cap = L.table_cap;
@@ -262,6 +264,7 @@ int tg_server_create(tg_context* ctx, const tg_server_params* p, void* d_arena,
   e = cudaStreamCreateWithFlags(&srv->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&srv->aux, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaMemsetAsync(srv->d_arena, 0, L.d_total, srv->aux);
+  if (e == cudaSuccess) e = cudaMemsetAsync(a.ring, 0xFF, size_t(L.Q) * 8, srv->aux);
   if (e == cudaSuccess && L.table_cap)
     e = cudaMemsetAsync(a.keys, 0xFF, L.table_cap * 8, srv->aux);
   if (e == cudaSuccess) e = cudaStreamSynchronize(srv->aux);
