@@ -619,8 +619,20 @@ def main(argv=None) -> None:
     ap.add_argument("--n-sets", type=int, default=N_SETS, help="sets per GPU (small cases)")
     ap.add_argument("--kmin", type=int, default=K_LO)
     ap.add_argument("--kmax", type=int, default=K_HI)
+    ap.add_argument("--section", choices=["canonical", "early-exit", "served"],
+                    help="run one secondary configuration alone and print its JSON")
+    ap.add_argument("--canon-n", type=int, default=1_000_000)
     args = ap.parse_args(argv)
     d = Dist()
+    if args.section:
+        from generalized_toric_gpu_search_b200 import build as lib_build
+
+        lib_build.build()
+        fn = {"canonical": lambda: bench_canonical(0, args.canon_n),
+              "early-exit": lambda: bench_early_exit(0),
+              "served": lambda: bench_served(0)}[args.section]
+        print(json.dumps({"section": args.section, **fn()}), flush=True)
+        return
     if args.impl == "reference":
         run_reference_arm(args, d)
         return

@@ -43,6 +43,10 @@ namespace tg {
 
 __constant__ uint8_t c_mul[64];
 __constant__ uint8_t c_inv[8];
+// Binomials C(n, r), n, r <= 20, and powers of 7 for the weight-ordered
+// enumeration of free head coefficients (task_start).
+__constant__ unsigned long long c_binom[21][21];
+__constant__ unsigned long long c_pow7[21];
 
 static bool g_tables_ready[64] = {false};
 
@@ -60,6 +64,16 @@ int upload_field_tables(int device) {
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyToSymbol(c_mul)");
   e = cudaMemcpyToSymbol(c_inv, inv, sizeof(inv));
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyToSymbol(c_inv)");
+  unsigned long long binom[21][21] = {}, pow7[21];
+  for (int n = 0; n <= 20; ++n) {
+    binom[n][0] = 1;
+    for (int r = 1; r <= n; ++r) binom[n][r] = binom[n - 1][r - 1] + (r <= n - 1 ? binom[n - 1][r] : 0);
+  }
+  pow7[0] = 1;
+  for (int i = 1; i <= 20; ++i) pow7[i] = pow7[i - 1] * 7ull;
+  e = cudaMemcpyToSymbol(c_binom, binom, sizeof(binom));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_pow7, pow7, sizeof(pow7));
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyToSymbol(c_binom)");
   g_tables_ready[device] = true;
   return TG_OK;
 }
@@ -422,11 +436,31 @@ __device__ __forceinline__ V6 task_start(const V6* B, uint32_t info, uint64_t q,
     for (int t = 0; t < 3; ++t)
       if (c2 >> t & 1) v6_xor(s, v6_load<kCG>(B + i2 * 3 + t));
   }
-  for (int r = H - 1; r >= ff; --r) {
-    const int dgt = int(q & 7ull);
-    q >>= 3;
-    for (int t = 0; t < 3; ++t)
-      if (dgt >> t & 1) v6_xor(s, v6_load<kCG>(B + r * 3 + t));
+  // Free rows ff..H-1 take every vector of GF(8)^F exactly once, ordered by
+  // the number of nonzero coefficients: light messages come first, so an
+  // early exit meets its witness sooner; the full set is unchanged.
+  const int F = H - ff;
+  int w = 0;
+  unsigned long long size = 1ull;  // C(F, 0) * 7^0
+  while (q >= size && w < F) {
+    q -= size;
+    ++w;
+    size = c_binom[F][w] * c_pow7[w];
+  }
+  unsigned long long comb = q / c_pow7[w];
+  unsigned long long dig = q - comb * c_pow7[w];
+  int rem = w;
+  for (int pos = F - 1; pos >= 0 && rem > 0; --pos) {
+    const unsigned long long b = c_binom[pos][rem];
+    if (comb >= b) {
+      comb -= b;
+      --rem;
+      const int dgt = int(dig % 7ull) + 1;
+      dig /= 7ull;
+      const int r = ff + pos;
+      for (int t = 0; t < 3; ++t)
+        if (dgt >> t & 1) v6_xor(s, v6_load<kCG>(B + r * 3 + t));
+    }
   }
   return s;
 }
