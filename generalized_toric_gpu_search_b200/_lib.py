@@ -72,6 +72,13 @@ SIGNATURES: dict[str, tuple] = {
     "tg_canonical_masks": (
         c_int, [c_void_p, c_void_p, c_int32, c_void_p, c_void_p, c_void_p, c_void_p]
     ),
+    "tg_expand_canonical": (c_int, [c_void_p, c_void_p, c_int32, c_void_p, c_void_p]),
+    "tg_compact_scratch_bytes": (c_int, [c_int32, POINTER(c_size_t)]),
+    "tg_compact_sets": (
+        c_int,
+        [c_void_p, c_void_p, c_int32, c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+         c_void_p],
+    ),
     "tg_hashset_bytes": (c_int, [c_int64, POINTER(c_size_t)]),
     "tg_hashset_clear": (c_int, [c_void_p, c_int64, c_void_p]),
     "tg_hashset_insert": (

@@ -405,6 +405,35 @@ int tg_canonical_masks(tg_context* ctx, const uint64_t* d_masks, int32_t n, uint
                        d_out_key_lo, d_out_key_hi, nullptr, static_cast<cudaStream_t>(stream));
 }
 
+int tg_expand_canonical(tg_context* ctx, const uint64_t* d_parents, int32_t n, uint64_t* d_out,
+                        void* stream) {
+  if (!ctx) return invalid("tg_expand_canonical: NULL context");
+  if (n < 0 || int64_t(n) * kN > int64_t(0x7fffffff))
+    return invalid("tg_expand_canonical: n must be >= 0 and n * 49 < 2^31");
+  if (n == 0) return TG_OK;
+  if (!d_parents || !d_out) return invalid("tg_expand_canonical: NULL device pointer");
+  DeviceGuard g(ctx->device);
+  if (g.error() != cudaSuccess) return cuda_fail(g.error(), "cudaSetDevice");
+  return run_canonical(ctx->device, ctx->sm_count, ctx->d_gl2, nullptr, d_parents, n * kN, 0,
+                       d_out, nullptr, nullptr, nullptr, static_cast<cudaStream_t>(stream), 1);
+}
+
+int tg_compact_scratch_bytes(int32_t n, size_t* h_bytes) {
+  if (!h_bytes || n < 0) return invalid("tg_compact_scratch_bytes: bad argument");
+  *h_bytes = compact_scratch_bytes(n);
+  return TG_OK;
+}
+
+int tg_compact_sets(const uint64_t* d_masks, const uint8_t* d_flags, int32_t n, int32_t k,
+                    void* d_scratch, uint64_t* d_out_masks, int32_t* d_out_sets,
+                    int64_t* d_out_offsets, int32_t* d_count, void* stream) {
+  if (n < 0 || k < 0 || k > kN) return invalid("tg_compact_sets: bad n or k");
+  if (!d_count || (n > 0 && (!d_masks || !d_flags || !d_scratch)))
+    return invalid("tg_compact_sets: NULL device pointer");
+  return run_compact(d_masks, d_flags, n, k, d_scratch, d_out_masks, d_out_sets, d_out_offsets,
+                     d_count, static_cast<cudaStream_t>(stream));
+}
+
 int tg_hashset_bytes(int64_t capacity, size_t* h_bytes) {
   if (!h_bytes) return invalid("tg_hashset_bytes: NULL output");
   if (capacity < 64 || (capacity & (capacity - 1)))

@@ -26,7 +26,8 @@ constexpr int kGl2Bytes = kGl2Order * kN;          // 98,784
 
 struct CanonArgs {
   const int32_t* sets;    // (n, k) rows, or NULL
-  const uint64_t* masks;  // n masks when sets == NULL
+  const uint64_t* masks;  // n masks when sets == NULL (parents when expand)
+  int expand;             // set s = parent s / 49 plus point s % 49 (0 if present)
   int n;
   int k;
   uint64_t* out_mask;
@@ -64,6 +65,10 @@ __global__ void __launch_bounds__(kCanonTPB, 2) canon_kernel(CanonArgs a) {
       const uint32_t hi = __reduce_or_sync(0xffffffffu, uint32_t(mine >> 32));
       S = uint64_t(lo) | (uint64_t(hi) << 32);
       bad = __any_sync(0xffffffffu, bad_a || bad_b) || __popcll(S) != k;
+    } else if (a.expand) {
+      const uint64_t parent = a.masks[s / kN] & kMask49;
+      const int p = s % kN;
+      S = (parent >> p & 1ull) ? 0ull : (parent | (1ull << p));
     } else {
       S = a.masks[s] & kMask49;
     }
@@ -114,7 +119,8 @@ static bool g_canon_attr[64] = {false};
 
 int run_canonical(int device, int sm_count, const uint8_t* d_gl2, const int32_t* d_sets,
                   const uint64_t* d_masks, int n, int k, uint64_t* d_out_mask,
-                  uint64_t* d_lo, uint64_t* d_hi, int32_t* d_status, cudaStream_t s) {
+                  uint64_t* d_lo, uint64_t* d_hi, int32_t* d_status, cudaStream_t s,
+                  int expand) {
   if (n <= 0) return TG_OK;
   if (!g_canon_attr[device]) {
     cudaError_t e = cudaFuncSetAttribute(canon_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -122,7 +128,7 @@ int run_canonical(int device, int sm_count, const uint8_t* d_gl2, const int32_t*
     if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(canon_kernel)");
     g_canon_attr[device] = true;
   }
-  CanonArgs a{d_sets, d_masks, n, k, d_out_mask, d_lo, d_hi, d_status, d_gl2};
+  CanonArgs a{d_sets, d_masks, expand, n, k, d_out_mask, d_lo, d_hi, d_status, d_gl2};
   const int warps_needed = n;
   int grid = sm_count * 2;
   const int max_grid = (warps_needed + (kCanonTPB / 32) - 1) / (kCanonTPB / 32);
@@ -165,10 +171,7 @@ __global__ void hash_insert_kernel(uint64_t* keys, uint64_t* tags, uint64_t cap,
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint64_t key = in[i];
-  if (key == kEmpty) {
-    if (status) atomicCAS(status, 0, TG_ERR_INVALID_ARGUMENT);
-    return;
-  }
+  if (key == kEmpty || key == 0ull) return;  // not a key: never new
   const unsigned long long tag = (static_cast<unsigned long long>(call_id) << 32) | uint32_t(i);
   uint64_t slot = hash_slot(key, cap);
   for (uint64_t probe = 0; probe < cap; ++probe) {
@@ -195,7 +198,7 @@ __global__ void hash_mark_kernel(const uint64_t* keys, const uint64_t* tags, uin
   bool fresh = false;
   if (i < n) {
     const uint64_t key = in[i];
-    if (key != kEmpty) {
+    if (key != kEmpty && key != 0ull) {
       const unsigned long long tag = (static_cast<unsigned long long>(call_id) << 32) | uint32_t(i);
       uint64_t slot = hash_slot(key, cap);
       for (uint64_t probe = 0; probe < cap; ++probe) {
@@ -217,6 +220,100 @@ __global__ void hash_mark_kernel(const uint64_t* keys, const uint64_t* tags, uin
 }
 
 size_t hashset_bytes(int64_t cap) { return 256 + size_t(cap) * 16; }
+
+// ---------------------------------------------------------------------------
+// Order-preserving compaction of flagged masks into sorted index rows.
+// ---------------------------------------------------------------------------
+
+constexpr int kCompactTPB = 256;
+
+__global__ void compact_count_kernel(const uint8_t* flags, int n, int* block_counts) {
+  __shared__ int s_cnt;
+  if (threadIdx.x == 0) s_cnt = 0;
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool f = i < n && flags[i];
+  const unsigned b = __ballot_sync(0xffffffffu, f);
+  if ((threadIdx.x & 31) == 0 && b) atomicAdd(&s_cnt, __popc(b));
+  __syncthreads();
+  if (threadIdx.x == 0) block_counts[blockIdx.x] = s_cnt;
+}
+
+__global__ void compact_scan_kernel(int* block_counts, int nb, int* total) {
+  // one thread: the number of blocks is n / 256 (a few tens of thousands)
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    int run = 0;
+    for (int b = 0; b < nb; ++b) {
+      const int c = block_counts[b];
+      block_counts[b] = run;
+      run += c;
+    }
+    *total = run;
+  }
+}
+
+__global__ void compact_write_kernel(const uint64_t* masks, const uint8_t* flags, int n, int k,
+                                     const int* block_offsets, uint64_t* out_masks,
+                                     int32_t* out_sets, int64_t* out_offsets) {
+  __shared__ int s_warp[kCompactTPB / 32];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const bool f = i < n && flags[i];
+  const unsigned b = __ballot_sync(0xffffffffu, f);
+  if (lane == 0) s_warp[w] = __popc(b);
+  __syncthreads();
+  int before = block_offsets[blockIdx.x];
+  for (int j = 0; j < w; ++j) before += s_warp[j];
+  before += __popc(b & ((1u << lane) - 1u));
+  if (f) {
+    const uint64_t m = masks[i];
+    if (out_masks) out_masks[before] = m;
+    if (out_sets) {
+      int32_t* row = out_sets + size_t(before) * size_t(k);
+      uint64_t x = m;
+      for (int j = 0; j < k; ++j) {
+        const int idx = x ? __ffsll(static_cast<long long>(x)) - 1 : 0;
+        x &= x - 1ull;
+        row[j] = idx;
+      }
+    }
+    if (out_offsets) {
+      out_offsets[before] = int64_t(before) * k;
+      out_offsets[before + 1] = int64_t(before + 1) * k;
+    }
+  }
+}
+
+size_t compact_scratch_bytes(int n) {
+  return size_t((n + kCompactTPB - 1) / kCompactTPB + 1) * sizeof(int);
+}
+
+int run_compact(const uint64_t* d_masks, const uint8_t* d_flags, int n, int k, void* d_scratch,
+                uint64_t* d_out_masks, int32_t* d_out_sets, int64_t* d_out_offsets,
+                int32_t* d_count, cudaStream_t s) {
+  if (n <= 0) {
+    cudaError_t e = cudaMemsetAsync(d_count, 0, sizeof(int32_t), s);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(count)");
+    if (d_out_offsets) {
+      e = cudaMemsetAsync(d_out_offsets, 0, sizeof(int64_t), s);
+      if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(offsets)");
+    }
+    return TG_OK;
+  }
+  const int nb = (n + kCompactTPB - 1) / kCompactTPB;
+  int* counts = static_cast<int*>(d_scratch);
+  compact_count_kernel<<<nb, kCompactTPB, 0, s>>>(d_flags, n, counts);
+  compact_scan_kernel<<<1, 32, 0, s>>>(counts, nb, d_count);
+  if (d_out_offsets) {
+    cudaError_t e = cudaMemsetAsync(d_out_offsets, 0, sizeof(int64_t), s);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(offsets)");
+  }
+  compact_write_kernel<<<nb, kCompactTPB, 0, s>>>(d_masks, d_flags, n, k, counts, d_out_masks,
+                                                   d_out_sets, d_out_offsets);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "compact kernels launch");
+  return TG_OK;
+}
 
 int run_hash_clear(void* table, int64_t cap, cudaStream_t s) {
   uint8_t* base = static_cast<uint8_t*>(table);

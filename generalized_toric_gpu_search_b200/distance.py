@@ -193,13 +193,36 @@ class DistanceOracleCUDABP:
 
     BLOCK_SIZE = 256  # kept for callers that read it; the B200 launch is persistent
 
-    def __init__(self, device_id: int, M: np.ndarray, config: LaunchConfig | None = None):
+    def __init__(self, device_id: int, M: np.ndarray, config: LaunchConfig | None = None,
+                 autotune: bool = True):
         self.device_id = device_id
         self.ctx = ToricContext(device_id, M)
-        self.runner = DistanceRunner(self.ctx, config)
+        self._fixed = config
+        self._table: dict = {}
+        if config is None and autotune:
+            from .autotune import load_table
+
+            self._table = load_table(_lib.device_info(device_id)[3])
+        self._runners: dict[tuple, DistanceRunner] = {}
+        self.runner = self._runner_for(0, False)
         self.device = self.runner.device
         self._stream = torch.cuda.Stream(device=self.device)
         self._lock = threading.Lock()
+
+    def _runner_for(self, k_max: int, sampled: bool) -> DistanceRunner:
+        """Launch shape: the fixed config, else the autotuned one for k_max."""
+        cfg = self._fixed
+        if cfg is None and not sampled and self._table:
+            from .autotune import choose
+
+            cfg = choose(self._table, k_max)
+        cfg = cfg or LaunchConfig()
+        key = (cfg.tail_rows, cfg.enumeration, cfg.variant, cfg.blocks_per_sm,
+               cfg.threads_per_block)
+        r = self._runners.get(key)
+        if r is None:
+            r = self._runners[key] = DistanceRunner(self.ctx, cfg)
+        return r
 
     # -- reference API --------------------------------------------------------
 
@@ -249,6 +272,7 @@ class DistanceOracleCUDABP:
                 if td_arr is not None:
                     d_td = torch.from_numpy(td_arr).pin_memory().to(self.device, non_blocking=True)
                 d_out = torch.empty(n, dtype=torch.int32, device=self.device)
+                self.runner = self._runner_for(k_max, sample_count > 0)
                 p = self.runner.params(n, k_max, 0 if per_set_td else int(target_distance),
                                        sample_count if sample_count > 0 else 0, sample_seed)
                 self.runner.run(p, d_idx, d_off, d_out, d_target=d_td, stream=s)
@@ -277,3 +301,40 @@ def init_cuda_oracles_bp(M: np.ndarray) -> tuple[list[DistanceOracleCUDABP], int
             sm_count = sm_i
         oracles.append(DistanceOracleCUDABP(i, M))
     return oracles, sm_count
+
+
+def dispatch_max_zeros_batch(oracles, batch, target_distance, sample_count: int = 0,
+                             sample_seed: int = 0) -> list[int]:
+    """A batch split over several oracles (one per GPU), as the reference's
+    _dispatch does (champion_search_canonical.py:237-271): near-even contiguous
+    chunks in device order, one host thread per device, and in sampled mode
+    the seed of device i offset by i * 1_000_003 so each chunk reproduces the
+    reference's per-device sampling.  Codes are independent, so there is no
+    exchange between devices; results come back in batch order."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    if not batch:
+        return []
+    n = len(oracles)
+
+    def call(o, chunk, seed):
+        if sample_count <= 0:
+            return o.max_zeros_batch(chunk, target_distance)
+        return o.max_zeros_batch(chunk, target_distance, sample_count=sample_count,
+                                 sample_seed=seed)
+
+    if n == 1:
+        return call(oracles[0], batch, sample_seed)
+    q, r = divmod(len(batch), n)
+    chunks, start = [], 0
+    for i in range(n):
+        size = q + (1 if i < r else 0)
+        chunks.append(batch[start:start + size])
+        start += size
+    with ThreadPoolExecutor(max_workers=n) as pool:
+        futs = [pool.submit(call, o, c, sample_seed + i * 1_000_003)
+                for i, (o, c) in enumerate(zip(oracles, chunks)) if c]
+        out: list[int] = []
+        for f in futs:
+            out.extend(f.result())
+    return out

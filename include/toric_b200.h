@@ -202,13 +202,34 @@ int tg_canonical_masks(tg_context* ctx, const uint64_t* d_masks, int32_t n,
                        uint64_t* d_out_mask, uint64_t* d_out_key_lo,
                        uint64_t* d_out_key_hi, void* stream);
 
+/* Canonical masks of all one-point extensions of n parent masks (49-bit):
+ * d_out[49 * i + p] = canonical mask of parent_i with point p added, or 0 when
+ * p is already in parent_i.  The expansion of the canonical BFS
+ * (champion_search_canonical.py:496-506) fused with its canonicalisation
+ * (kernel_canon.py:151-176), on the device.  n * 49 must fit in int32. */
+int tg_expand_canonical(tg_context* ctx, const uint64_t* d_parents, int32_t n,
+                        uint64_t* d_out, void* stream);
+
+/* Scratch bytes of tg_compact_sets for n entries. */
+int tg_compact_scratch_bytes(int32_t n, size_t* h_bytes);
+/* Order-preserving compaction of the entries i with d_flags[i] != 0: their
+ * masks (d_out_masks, may be NULL), their sorted exponent indices as rows of
+ * k int32 (d_out_sets, may be NULL; each mask must hold k points) and
+ * count+1 row offsets (d_out_offsets, may be NULL); *d_count = count.  Feeds
+ * a level of new canonical sets straight into tg_max_zeros. */
+int tg_compact_sets(const uint64_t* d_masks, const uint8_t* d_flags, int32_t n,
+                    int32_t k, void* d_scratch, uint64_t* d_out_masks,
+                    int32_t* d_out_sets, int64_t* d_out_offsets, int32_t* d_count,
+                    void* stream);
+
 /* ---- device hash set (canonical dedup) ----------------------------------- */
 
 /* Bytes of a hash set with `capacity` slots (power of two >= 64). */
 int tg_hashset_bytes(int64_t capacity, size_t* h_bytes);
 /* Empties a hash set. */
 int tg_hashset_clear(void* d_table, int64_t capacity, void* stream);
-/* Inserts n 64-bit keys (any value but all ones).  d_is_new[i] = 1 iff key i
+/* Inserts n 64-bit keys; 0 and all ones are not keys (never new, not stored).
+ * d_is_new[i] = 1 iff key i
  * was absent before this call and i is its first index in this call — the
  * semantics of the reference's `seen` set walk in
  * champion_search_canonical.py:337-345.  `call_id` must grow from call to
