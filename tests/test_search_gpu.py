@@ -61,7 +61,7 @@ def test_bfs_pruned_with_targets(M):
 
 
 def test_autotune_small_table(tmp_path, gpu_oracle):
-    from generalized_toric_gpu_search_b200 import autotune
+    from generalized_toric_gpu_search_b200 import _lib, autotune
     from generalized_toric_gpu_search_b200.distance import DistanceOracleCUDABP
     from generalized_toric_gpu_search_b200.tables import build_eval_matrix
 
@@ -70,9 +70,7 @@ def test_autotune_small_table(tmp_path, gpu_oracle):
              dict(tail_rows=4, blocks_per_sm=8, threads_per_block=128)]
     table = autotune.tune(0, ks=[9], candidates=cands, path=path)
     assert set(table) == {9} and table[9]["tail_rows"] in (3, 4)
-    cfg = autotune.choose(autotune.load_table(
-        __import__("generalized_toric_gpu_search_b200._lib", fromlist=["x"]).device_info(0)[3],
-        path), 9)
+    cfg = autotune.choose(autotune.load_table(_lib.device_info(0)[3], path), 9)
     o = DistanceOracleCUDABP(0, build_eval_matrix(), config=cfg)
     sets = autotune.calibration_sets(9)[:50]
     assert o.max_zeros_batch(sets, 1) == gpu_oracle.max_zeros_batch(sets, 1)
