@@ -28,6 +28,8 @@ TG_ERR_STATE = 8
 TG_ENUM_AUTO = 0
 TG_ENUM_PROJECTIVE = 1
 TG_ENUM_ORBIT = 2
+TG_ENUM_INFOSET = 3
+TG_INFOSET_AUTO_MIN_K = 10
 TG_VARIANT_AUTO = 0
 TG_VARIANT_HISTOGRAM = 1
 TG_VARIANT_DIRECT = 2

@@ -214,7 +214,7 @@ static int check_distance_params(const tg_distance_params* p) {
   }
   if (p->tail_rows != 0 && (p->tail_rows < 2 || p->tail_rows > 7))
     return invalid("tail_rows must be 0 or 2..7");
-  if (p->enumeration < TG_ENUM_AUTO || p->enumeration > TG_ENUM_ORBIT)
+  if (p->enumeration < TG_ENUM_AUTO || p->enumeration > TG_ENUM_INFOSET)
     return invalid("unknown enumeration");
   if (p->variant < TG_VARIANT_AUTO || p->variant > TG_VARIANT_DIRECT)
     return invalid("unknown variant");
@@ -246,6 +246,15 @@ static void bind_workspace(DistArgs& a, const WsLayout& L, void* ws) {
   a.basis_stride = L.basis_stride;
   a.pat_stride = L.pat_stride;
   a.bitpat_stride = L.bitpat_stride;
+  a.is_min_k = L.is_min_k;
+  a.is_stride = L.is_stride;
+  a.is_hdr = reinterpret_cast<WsHeader*>(b + L.is_hdr);
+  a.is_rows = reinterpret_cast<V6*>(b + L.is_rows);
+  a.is_cnt = reinterpret_cast<uint64_t*>(b + L.is_cnt);
+  a.is_off = reinterpret_cast<uint64_t*>(b + L.is_off);
+  a.is_done = reinterpret_cast<unsigned long long*>(b + L.is_done);
+  a.is_best = reinterpret_cast<int32_t*>(b + L.is_best);
+  a.is_bits = reinterpret_cast<uint32_t*>(b + L.is_bits);
 }
 
 // Validates a max_zeros call and fills the kernel arguments.
@@ -266,8 +275,10 @@ static int bind_distance(tg_context* ctx, const tg_distance_params* p, const int
     set_last_error("tg_max_zeros: workspace has %zu bytes, needs %zu", workspace_bytes, L.total);
     return TG_ERR_WORKSPACE;
   }
+  // Enumeration of the codes below the information-set threshold.
   int enumeration = p->enumeration;
   if (enumeration == TG_ENUM_AUTO) enumeration = ctx->is_toric ? TG_ENUM_ORBIT : TG_ENUM_PROJECTIVE;
+  if (enumeration == TG_ENUM_INFOSET) enumeration = TG_ENUM_PROJECTIVE;
   if (enumeration == TG_ENUM_ORBIT && !ctx->is_toric)
     return invalid("orbit enumeration needs the toric evaluation matrix");
   int variant = p->variant;
@@ -369,9 +380,13 @@ int tg_distance_counters(const tg_distance_params* p, const void* d_workspace, v
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   cudaError_t e = cudaMemcpyAsync(&h, static_cast<const uint8_t*>(d_workspace) + L.hdr, sizeof(h),
                                   cudaMemcpyDeviceToHost, s);
+  WsHeader hi{};
+  if (e == cudaSuccess && L.is_min_k <= p->k_max && p->n_sets > 0)
+    e = cudaMemcpyAsync(&hi, static_cast<const uint8_t*>(d_workspace) + L.is_hdr, sizeof(hi),
+                        cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_fail(e, "tg_distance_counters");
-  if (h_tasks) *h_tasks = h.total_tasks;
+  if (h_tasks) *h_tasks = h.total_tasks + hi.total_tasks;
   if (h_codewords) *h_codewords = h.codewords;
   if (h_reference_messages) *h_reference_messages = h.ref_messages;
   return TG_OK;

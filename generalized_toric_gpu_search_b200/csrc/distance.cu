@@ -33,6 +33,7 @@
 //    14 LOP3 + 14 POPC.
 //  * Direct variant (any M).  One OR of the three planes and two POPC per
 //    codeword.
+#include <algorithm>
 #include <cstdio>
 
 #include "common.cuh"
@@ -43,10 +44,11 @@ namespace tg {
 
 __constant__ uint8_t c_mul[64];
 __constant__ uint8_t c_inv[8];
-// Binomials C(n, r), n, r <= 20, and powers of 7 for the weight-ordered
-// enumeration of free head coefficients (task_start).
-__constant__ unsigned long long c_binom[21][21];
-__constant__ unsigned long long c_pow7[21];
+// Binomials C(n, r), n, r <= 21 (0 for r > n), and powers of 7 for the
+// weight-ordered enumeration of free head coefficients (task_start) and the
+// information-set levels.
+__constant__ unsigned long long c_binom[22][22];
+__constant__ unsigned long long c_pow7[22];
 
 static bool g_tables_ready[64] = {false};
 
@@ -64,13 +66,13 @@ int upload_field_tables(int device) {
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyToSymbol(c_mul)");
   e = cudaMemcpyToSymbol(c_inv, inv, sizeof(inv));
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyToSymbol(c_inv)");
-  unsigned long long binom[21][21] = {}, pow7[21];
-  for (int n = 0; n <= 20; ++n) {
+  unsigned long long binom[22][22] = {}, pow7[22];
+  for (int n = 0; n <= 21; ++n) {
     binom[n][0] = 1;
     for (int r = 1; r <= n; ++r) binom[n][r] = binom[n - 1][r - 1] + (r <= n - 1 ? binom[n - 1][r] : 0);
   }
   pow7[0] = 1;
-  for (int i = 1; i <= 20; ++i) pow7[i] = pow7[i - 1] * 7ull;
+  for (int i = 1; i <= 21; ++i) pow7[i] = pow7[i - 1] * 7ull;
   e = cudaMemcpyToSymbol(c_binom, binom, sizeof(binom));
   if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_pow7, pow7, sizeof(pow7));
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyToSymbol(c_binom)");
@@ -93,6 +95,25 @@ int default_tail_rows(const tg_distance_params& p) {
   return p.tail_rows > 0 ? p.tail_rows : 4;
 }
 
+// Smallest k evaluated by information sets (kNever: none).
+constexpr int kNever = 1 << 20;
+int infoset_min_k(const tg_distance_params& p) {
+  if (p.sample_count > 0) return kNever;
+  if (p.enumeration == TG_ENUM_INFOSET) return 2;
+  if (p.enumeration == TG_ENUM_AUTO) return TG_INFOSET_AUTO_MIN_K;
+  return kNever;
+}
+
+// Rows (sets x k) an information-set code of k_lo <= k <= k_hi may store.
+static int infoset_rows(int k_lo, int k_hi) {
+  int rows = 0;
+  for (int k = k_lo; k <= k_hi; ++k) {
+    const int sets = std::min(8, 64 / k);  // kIsMaxSets, kIsMaxRows
+    rows = std::max(rows, sets * k);
+  }
+  return rows;
+}
+
 WsLayout ws_layout(const tg_distance_params& p) {
   WsLayout L{};
   const size_t n = size_t(p.n_sets > 0 ? p.n_sets : 0);
@@ -112,6 +133,17 @@ WsLayout ws_layout(const tg_distance_params& p) {
   L.pat_cum = off;  off = align256(off + n * size_t(L.pat_stride) * sizeof(uint64_t));
   L.pat_info = off; off = align256(off + n * size_t(L.pat_stride) * sizeof(uint32_t));
   L.bitpat = off;   off = align256(off + n * size_t(L.bitpat_stride) * sizeof(V6));
+  L.is_min_k = infoset_min_k(p);
+  const bool infoset = L.is_min_k <= kmax;
+  const size_t levels = infoset ? n * size_t(kmax) : 0;
+  L.is_stride = infoset ? infoset_rows(L.is_min_k, kmax) * 7 : 0;  // kIsVecPerRow
+  L.is_hdr = off;   off = align256(off + (infoset ? sizeof(WsHeader) : 0));
+  L.is_rows = off;  off = align256(off + n * size_t(L.is_stride) * sizeof(V6));
+  L.is_cnt = off;   off = align256(off + levels * sizeof(uint64_t));
+  L.is_off = off;   off = align256(off + (infoset ? levels + 1 : 0) * sizeof(uint64_t));
+  L.is_done = off;  off = align256(off + levels * sizeof(uint64_t));
+  L.is_best = off;  off = align256(off + (infoset ? n : 0) * sizeof(int32_t));
+  L.is_bits = off;  off = align256(off + (infoset ? n : 0) * sizeof(uint32_t));
   L.total = off;
   return L;
 }
@@ -325,6 +357,16 @@ prep_exact_kernel(DistArgs a) {
   }
   if (lane < 32) s_idx[w][lane] = my;
   __syncwarp();
+  if (ok && k >= a.is_min_k) {
+    // Evaluated by information sets (prep_infoset_kernel fills the rest).
+    if (lane == 0) {
+      d.k = k;
+      d.flags = kIsCodeFlag;
+      d.n_tasks = 0ull;
+      a.desc[c] = d;
+    }
+    return;
+  }
   PrepResult pr{0, 0ull, 0, 0, 0};
   if (ok) {
     V6* B = a.basis + size_t(c) * a.basis_stride;
@@ -781,9 +823,17 @@ __global__ void __launch_bounds__(kTPB) walk_sampled_kernel(DistArgs a) {
   }
 }
 
+}  // namespace tg
+
+#include "infoset_kernel.cuh"
+
+namespace tg {
+
 // ---------------------------------------------------------------------------
 // Host launcher
 // ---------------------------------------------------------------------------
+
+constexpr int kIsWalkThreads = 128;
 
 // Two register budgets per CTA shape: 1024 resident threads per SM (64
 // registers per thread) or 512 (128 registers).
@@ -815,6 +865,15 @@ int run_prepare(const DistArgs& args, cudaStream_t s) {
   else prep_exact_kernel<<<prep_grid, kPrepWarps * 32, 0, s>>>(args);
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "prep kernel launch");
+  if (args.is_min_k <= args.k_max) {
+    e = cudaMemsetAsync(args.is_hdr, 0, sizeof(WsHeader), s);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(information-set header)");
+    prep_infoset_kernel<<<(args.n + kIsPrepWarps - 1) / kIsPrepWarps, kIsPrepWarps * 32, 0, s>>>(
+        args);
+    scan_levels_kernel<<<1, kScanThreads, 0, s>>>(args);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "information-set prep launch");
+  }
   scan_tasks_kernel<<<1, kScanThreads, 0, s>>>(args);
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "scan kernel launch");
@@ -832,6 +891,14 @@ int run_walk(const DistArgs& args, int sm_count, int blocks_per_sm, int tpb, cud
     default: e = launch_walk<128>(args.variant, sampled, grid, blocks_per_sm, args, s); break;
   }
   if (e != cudaSuccess) return cuda_fail(e, "walk kernel launch");
+  if (args.is_min_k <= args.k_max) {
+    // Information-set walk: 512 resident threads per SM (128 registers).
+    walk_infoset_kernel<kIsWalkThreads, 512 / kIsWalkThreads>
+        <<<sm_count * (512 / kIsWalkThreads), kIsWalkThreads, 0, s>>>(args);
+    finalize_infoset_kernel<<<(args.n + 255) / 256, 256, 0, s>>>(args);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "information-set walk launch");
+  }
   return TG_OK;
 }
 

@@ -27,10 +27,16 @@ struct CodeDesc {
   int32_t pad;
   uint64_t n_tasks; // tasks of this code
 };
+// Information-set codes reuse the descriptor: R = full sets, H = all sets,
+// n_pat = rank deficit of the partial set (0 when there is none).
+
+constexpr int32_t kDecidedFlag = 1;  // value known after preparation
+constexpr int32_t kIsCodeFlag = 2;   // evaluated by information sets
 
 struct WsLayout {
-  size_t hdr, desc, task_off, abort, basis, pat_cum, pat_info, bitpat, total;
-  int basis_stride, pat_stride, bitpat_stride;
+  size_t hdr, desc, task_off, abort, basis, pat_cum, pat_info, bitpat;
+  size_t is_hdr, is_rows, is_cnt, is_off, is_done, is_best, is_bits, total;
+  int basis_stride, pat_stride, bitpat_stride, is_stride, is_min_k;
 };
 
 struct DistArgs {
@@ -42,7 +48,7 @@ struct DistArgs {
   int n;
   int k_max;
   int R;
-  int enumeration;   // TG_ENUM_PROJECTIVE or TG_ENUM_ORBIT
+  int enumeration;   // TG_ENUM_PROJECTIVE or TG_ENUM_ORBIT (codes with k < is_min_k)
   int variant;       // TG_VARIANT_HISTOGRAM or TG_VARIANT_DIRECT
   int td_default;
   int64_t sample_count;
@@ -58,12 +64,23 @@ struct DistArgs {
   int basis_stride;
   int pat_stride;
   int bitpat_stride;
+  // Information-set path: codes with is_min_k <= k (is_min_k > k_max: none).
+  int is_min_k;
+  int is_stride;                 // V6 per code in is_rows
+  WsHeader* is_hdr;              // task queue of the information-set walk
+  V6* is_rows;                   // per code and set: k rows x (g, 6 deltas)
+  uint64_t* is_cnt;              // tasks per (level, code), level-major
+  uint64_t* is_off;              // exclusive scan of is_cnt (n * k_max + 1)
+  unsigned long long* is_done;   // finished tasks per (level, code)
+  int32_t* is_best;              // smallest weight met per code
+  uint32_t* is_bits;             // completed levels per code (bit w - 1)
   DeviceTables tab;
 };
 
 int upload_field_tables(int device);
 int max_patterns(int H);
 int default_tail_rows(const tg_distance_params& p);
+int infoset_min_k(const tg_distance_params& p);
 WsLayout ws_layout(const tg_distance_params& p);
 int run_prepare(const DistArgs& args, cudaStream_t s);
 int run_walk(const DistArgs& args, int sm_count, int blocks_per_sm, int tpb, cudaStream_t s);

@@ -82,11 +82,24 @@ int tg_context_is_toric(const tg_context* ctx, int32_t* h_is_toric);
 
 /* ---- max_zeros (exact and sampled) -------------------------------------- */
 
+/* Exact enumeration strategies.  All give the same max_zeros (and the same
+ * pass/fail decision under an early exit); they differ in how many codewords
+ * they evaluate.
+ *   AUTO        sets with k >= TG_INFOSET_AUTO_MIN_K by information sets, the
+ *               others by orbit (toric context) or projective enumeration
+ *   PROJECTIVE  every message whose first nonzero coefficient is 1
+ *   ORBIT       projective + torus-orbit normalisation (toric context only)
+ *   INFOSET     information sets (Brouwer-Zimmermann) for every set, k >= 2:
+ *               messages of weight 1, 2, ... on disjoint information sets,
+ *               stopping when the weight bound of the unseen codewords
+ *               reaches the best weight found; any evaluation matrix */
 enum {
-  TG_ENUM_AUTO = 0,       /* orbit when the context is toric, else projective */
-  TG_ENUM_PROJECTIVE = 1, /* messages whose first nonzero coefficient is 1    */
-  TG_ENUM_ORBIT = 2       /* projective + torus-orbit normalisation (toric M) */
+  TG_ENUM_AUTO = 0,
+  TG_ENUM_PROJECTIVE = 1,
+  TG_ENUM_ORBIT = 2,
+  TG_ENUM_INFOSET = 3
 };
+#define TG_INFOSET_AUTO_MIN_K 10
 enum {
   TG_VARIANT_AUTO = 0,      /* histogram when the context is toric            */
   TG_VARIANT_HISTOGRAM = 1, /* last row via an 8-bin zero histogram           */
@@ -174,8 +187,9 @@ int tg_distance_status(const tg_distance_params* p, const void* d_workspace,
                        void* stream, int32_t* h_status);
 
 /* Work accounting of the last run on this workspace (synchronises `stream`):
- * tasks launched, codewords evaluated (sum over tasks) and the
- * reference-equivalent message count sum(8^k - 1) over exact sets. */
+ * tasks queued, codewords evaluated (orbit / projective: the codewords the
+ * queued tasks cover; information sets: the codewords the walk evaluated) and
+ * the reference-equivalent message count sum(8^k - 1) over exact sets. */
 int tg_distance_counters(const tg_distance_params* p, const void* d_workspace,
                          void* stream, uint64_t* h_tasks,
                          uint64_t* h_codewords, double* h_reference_messages);

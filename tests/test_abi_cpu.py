@@ -64,6 +64,18 @@ def test_workspace_size_and_validation(lib):
     assert _ws(lib, n_sets=1, k_max=3, tail_rows=1)[0] == _lib.TG_ERR_INVALID_ARGUMENT
     assert _ws(lib, n_sets=1, k_max=3, threads_per_block=96)[0] == _lib.TG_ERR_INVALID_ARGUMENT
     assert "k <= 21" in _lib.last_error() or "threads_per_block" in _lib.last_error()
+    assert _ws(lib, n_sets=1, k_max=3, enumeration=4)[0] == _lib.TG_ERR_INVALID_ARGUMENT
+    assert "enumeration" in _lib.last_error()
+    # information-set sections: none for orbit-only runs, none for AUTO below
+    # its threshold
+    st_o, orbit_b = _ws(lib, n_sets=1000, k_max=14, enumeration=_lib.TG_ENUM_ORBIT)
+    st_i, infoset_b = _ws(lib, n_sets=1000, k_max=14, enumeration=_lib.TG_ENUM_INFOSET)
+    st_a, auto_b = _ws(lib, n_sets=1000, k_max=14)
+    assert st_o == st_i == st_a == 0
+    assert infoset_b > orbit_b + 1000 * 14 * 8 * 3 and auto_b > orbit_b
+    below = _lib.TG_INFOSET_AUTO_MIN_K - 1
+    assert _ws(lib, n_sets=1000, k_max=below)[1] == \
+        _ws(lib, n_sets=1000, k_max=below, enumeration=_lib.TG_ENUM_ORBIT)[1]
 
 
 def test_hashset_validation(lib):
