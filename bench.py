@@ -40,6 +40,10 @@ METRIC = "GF(8) codewords/s, reference-equivalent (8^k-1 messages per code), bat
 UNIT = "codewords/s"
 WORKLOAD = "batched uneven evaluation: 10,000 seeded random P, |P|~U{6..14}, td=1, exact"
 POPC_PER_CODEWORD = 14.0 / 8.0  # histogram walk: 7 bins x 2 words per 8 codewords
+POPC_PER_CODEWORD_INFOSET = 2.0  # information-set walk: one weight per codeword
+# Kernels per step: prep_exact, prep_infoset, scan_levels, scan_tasks,
+# walk_hist, walk_infoset, finalize_infoset.
+LAUNCHES_PER_STEP = 7
 L2_FLUSH_BYTES = 256 << 20
 
 
@@ -459,19 +463,24 @@ def run_b200_arm(args, d: Dist) -> None:
     stream = torch.cuda.Stream(device=device)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=device)
 
-    # Two CUDA graphs: prepare (header reset, prep, scan) and the persistent walk.
-    g_prep, g_walk = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
+    # Three CUDA graphs: prepare (header resets, prep, scans), the enumeration
+    # walk (sets below the information-set threshold) and the information-set
+    # walk, so each walk is timed by its own events.
+    g_prep, g_enum, g_is = (torch.cuda.CUDAGraph() for _ in range(3))
     with torch.cuda.stream(stream):
         runner.run(p, d_idx, d_off, d_out, stream=stream, workspace=ws)  # warm the module
     stream.synchronize()
     with torch.cuda.graph(g_prep, stream=stream, capture_error_mode="thread_local"):
         runner.prepare(p, d_idx, d_off, d_out, stream=stream, workspace=ws)
-    with torch.cuda.graph(g_walk, stream=stream, capture_error_mode="thread_local"):
-        runner.walk(p, d_out, stream=stream, workspace=ws)
+    with torch.cuda.graph(g_enum, stream=stream, capture_error_mode="thread_local"):
+        runner.walk(p, d_out, stream=stream, workspace=ws, parts=_lib.TG_WALK_ENUMERATION)
+    with torch.cuda.graph(g_is, stream=stream, capture_error_mode="thread_local"):
+        runner.walk(p, d_out, stream=stream, workspace=ws, parts=_lib.TG_WALK_INFOSET)
 
     def step():
         g_prep.replay()
-        g_walk.replay()
+        g_enum.replay()
+        g_is.replay()
 
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
@@ -479,8 +488,9 @@ def run_b200_arm(args, d: Dist) -> None:
     stream.synchronize()
     check = d_out.cpu().tolist()
     tasks, codewords, ref_msgs = runner.counters(stream)
+    paths = runner.path_counters(stream)
 
-    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
     clocks = ClockSampler(dev)
     d.barrier()
     torch.cuda.synchronize()
@@ -491,14 +501,18 @@ def run_b200_arm(args, d: Dist) -> None:
             ev[i][0].record(stream)
             g_prep.replay()
             ev[i][1].record(stream)
-            g_walk.replay()
+            g_enum.replay()
             ev[i][2].record(stream)
+            g_is.replay()
+            ev[i][3].record(stream)
     stream.synchronize()
     torch.cuda.synchronize()
     clk = clocks.stop()
     d.barrier()
-    step_ms = [e[0].elapsed_time(e[2]) for e in ev]
-    walk_ms = [e[1].elapsed_time(e[2]) for e in ev]
+    step_ms = [e[0].elapsed_time(e[3]) for e in ev]
+    prep_ms = [e[0].elapsed_time(e[1]) for e in ev]
+    enum_ms = [e[1].elapsed_time(e[2]) for e in ev]
+    is_ms = [e[2].elapsed_time(e[3]) for e in ev]
     if d_out.cpu().tolist() != check:
         raise SystemExit("results changed between steps")
     total_ms = d.max(sum(step_ms), device)
@@ -547,13 +561,24 @@ def run_b200_arm(args, d: Dist) -> None:
         plain = {"value": ref_msgs / plain_s, "unit": UNIT, "codes_per_s": len(sets) / plain_s,
                  "sample": "4 sets per k, one launch per set, per-k mean time x k histogram"}
 
-    # Roofline of the dominant kernel (the persistent histogram walk).
+    # Roofline of the dominant kernel: the walk with the larger share of the
+    # step, on the POPC pipe that bounds both walks.
     pipes = measure_pipes(dev) if d.rank == 0 else {}
-    walk_s = statistics.mean(walk_ms) / 1e3
     sm_count = ctx.sm_count
     mhz = clk.get("sm_mhz") or pipes.get("ubench_sm_mhz")
-    achieved = POPC_PER_CODEWORD * codewords / walk_s
     peak = pipes.get("popc_per_clk_sm", 16.0) * sm_count * (mhz or 1965.0) * 1e6
+    enum_s, is_s = statistics.mean(enum_ms) / 1e3, statistics.mean(is_ms) / 1e3
+    if is_s >= enum_s:
+        dominant = {"kernel": "walk_infoset_kernel (+ finalize_infoset_kernel)",
+                    "seconds": is_s, "codewords": paths["infoset_codewords"],
+                    "popc_per_codeword": POPC_PER_CODEWORD_INFOSET,
+                    "note": "2 POPC per codeword (one per 32-bit half of the nonzero mask)"}
+    else:
+        dominant = {"kernel": "walk_hist_kernel", "seconds": enum_s,
+                    "codewords": paths["enumeration_codewords"],
+                    "popc_per_codeword": POPC_PER_CODEWORD,
+                    "note": "1.75 POPC per codeword (14 per 8-codeword histogram)"}
+    achieved = dominant["popc_per_codeword"] * dominant["codewords"] / dominant["seconds"]
 
     extra = {}
     if d.rank == 0 and not args.skip_extra:
@@ -574,24 +599,27 @@ def run_b200_arm(args, d: Dist) -> None:
             "data": "synthetic (seeded random exponent sets)",
             "config": {"workload": WORKLOAD, "n_sets_per_gpu": len(sets),
                        "k_range": [K_LO, K_HI], "target_distance": 1,
-                       "enumeration": "orbit (projective + torus normalisation)",
+                       "enumeration": "auto: information sets for k >= 10, orbit "
+                                      "(projective + torus normalisation) below",
                        "variant": "histogram", "tail_rows": args.tail_rows or 4,
-                       "launch": "CUDA graphs: prepare + one persistent walk",
+                       "launch": "CUDA graphs: prepare, enumeration walk, information-set walk",
                        "l2": "256 MiB write between timed steps",
                        "parallelism": f"weak, {d.world} rank(s), no data-path collective"},
             "codes_per_s": d.world * len(sets) / (total_ms / 1e3 / args.steps),
             "evaluated_codewords_per_s": d.world * codewords / (total_ms / 1e3 / args.steps),
-            "evaluated_codewords_per_step": codewords, "tasks_per_step": tasks,
-            "walk_ms": statistics.mean(walk_ms),
+            "evaluated_codewords_per_step": codewords, "path_counters": paths,
+            "prep_ms": statistics.mean(prep_ms), "enumeration_walk_ms": statistics.mean(enum_ms),
+            "infoset_walk_ms": statistics.mean(is_ms),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * e2e_max / args.steps,
                     "api": "DistanceOracleCUDABP.max_zeros_batch(list of lists, 1)"},
-            "gpu_launches": 3 * args.steps,
+            "gpu_launches": LAUNCHES_PER_STEP * args.steps,
             "roofline": {"bound": "int (POPC pipe)", "achieved": achieved / 1e12,
                          "peak": peak / 1e12, "unit": "Tpopc/s", "frac": achieved / peak,
-                         "traffic": None,
-                         "note": "1.75 POPC per codeword (14 per 8-codeword histogram); peak = "
-                                 "measured POPC/clk/SM x SMs x median SM MHz in the timed region"},
+                         "traffic": None, "kernel": dominant["kernel"],
+                         "kernel_share": dominant["seconds"] / (statistics.mean(step_ms) / 1e3),
+                         "note": dominant["note"] + "; peak = measured POPC/clk/SM x SMs x "
+                                 "median SM MHz in the timed region"},
             "int_pipes": pipes,
             "clocks": clk,
             "plain_form": plain,
@@ -600,7 +628,7 @@ def run_b200_arm(args, d: Dist) -> None:
             **extra,
         }
         print(json.dumps(line), flush=True)
-    del g_prep, g_walk
+    del g_prep, g_enum, g_is
     d.close()
 
 

@@ -30,6 +30,8 @@ TG_ENUM_PROJECTIVE = 1
 TG_ENUM_ORBIT = 2
 TG_ENUM_INFOSET = 3
 TG_INFOSET_AUTO_MIN_K = 10
+TG_WALK_ENUMERATION = 1
+TG_WALK_INFOSET = 2
 TG_VARIANT_AUTO = 0
 TG_VARIANT_HISTOGRAM = 1
 TG_VARIANT_DIRECT = 2
@@ -59,6 +61,9 @@ SIGNATURES: dict[str, tuple] = {
          c_size_t, c_void_p],
     ),
     "tg_max_zeros_walk": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
+    "tg_max_zeros_walk_part": (
+        c_int, [c_void_p, c_void_p, c_int32, c_void_p, c_void_p, c_size_t, c_void_p]
+    ),
     "tg_max_zeros_noalloc": (
         c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]
     ),
@@ -67,6 +72,7 @@ SIGNATURES: dict[str, tuple] = {
         c_int,
         [c_void_p, c_void_p, c_void_p, POINTER(c_uint64), POINTER(c_uint64), POINTER(c_double)],
     ),
+    "tg_distance_path_counters": (c_int, [c_void_p, c_void_p, c_void_p, POINTER(c_uint64)]),
     "tg_canonical_sets": (
         c_int,
         [c_void_p, c_void_p, c_int32, c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p],

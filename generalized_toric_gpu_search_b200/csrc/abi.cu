@@ -324,8 +324,11 @@ int tg_max_zeros_prepare(tg_context* ctx, const tg_distance_params* p, const int
   return run_prepare(a, static_cast<cudaStream_t>(stream));
 }
 
-int tg_max_zeros_walk(tg_context* ctx, const tg_distance_params* p, int32_t* d_out,
-                      void* d_workspace, size_t workspace_bytes, void* stream) {
+int tg_max_zeros_walk_part(tg_context* ctx, const tg_distance_params* p, int32_t parts,
+                           int32_t* d_out, void* d_workspace, size_t workspace_bytes,
+                           void* stream) {
+  if (parts < 1 || parts > (TG_WALK_ENUMERATION | TG_WALK_INFOSET))
+    return invalid("tg_max_zeros_walk_part: parts must be a nonempty mask of TG_WALK_*");
   DistArgs a;
   int st = bind_distance(ctx, p, nullptr, nullptr, nullptr, nullptr, d_out, d_workspace,
                          workspace_bytes, false, a);
@@ -334,7 +337,15 @@ int tg_max_zeros_walk(tg_context* ctx, const tg_distance_params* p, int32_t* d_o
   if (g.error() != cudaSuccess) return cuda_fail(g.error(), "cudaSetDevice");
   int bps, tpb;
   launch_shape(p, &bps, &tpb);
-  return run_walk(a, ctx->sm_count, bps, tpb, static_cast<cudaStream_t>(stream));
+  return run_walk(a, ctx->sm_count, bps, tpb, static_cast<cudaStream_t>(stream),
+                  (parts & TG_WALK_ENUMERATION ? kWalkEnumeration : 0) |
+                      (parts & TG_WALK_INFOSET ? kWalkInfoset : 0));
+}
+
+int tg_max_zeros_walk(tg_context* ctx, const tg_distance_params* p, int32_t* d_out,
+                      void* d_workspace, size_t workspace_bytes, void* stream) {
+  return tg_max_zeros_walk_part(ctx, p, TG_WALK_ENUMERATION | TG_WALK_INFOSET, d_out,
+                                d_workspace, workspace_bytes, stream);
 }
 
 int tg_max_zeros(tg_context* ctx, const tg_distance_params* p, const int32_t* d_indices,
@@ -387,8 +398,29 @@ int tg_distance_counters(const tg_distance_params* p, const void* d_workspace, v
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_fail(e, "tg_distance_counters");
   if (h_tasks) *h_tasks = h.total_tasks + hi.total_tasks;
-  if (h_codewords) *h_codewords = h.codewords;
+  if (h_codewords) *h_codewords = h.codewords + hi.codewords;
   if (h_reference_messages) *h_reference_messages = h.ref_messages;
+  return TG_OK;
+}
+
+int tg_distance_path_counters(const tg_distance_params* p, const void* d_workspace, void* stream,
+                              uint64_t* h_counts) {
+  int st = check_distance_params(p);
+  if (st) return st;
+  if (!d_workspace || !h_counts) return invalid("tg_distance_path_counters: NULL argument");
+  const WsLayout L = ws_layout(*p);
+  WsHeader h{}, hi{};
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const uint8_t* b = static_cast<const uint8_t*>(d_workspace);
+  cudaError_t e = cudaMemcpyAsync(&h, b + L.hdr, sizeof(h), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess && L.is_min_k <= p->k_max && p->n_sets > 0)
+    e = cudaMemcpyAsync(&hi, b + L.is_hdr, sizeof(hi), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(e, "tg_distance_path_counters");
+  h_counts[0] = h.total_tasks;
+  h_counts[1] = h.codewords;
+  h_counts[2] = hi.total_tasks;
+  h_counts[3] = hi.codewords;
   return TG_OK;
 }
 

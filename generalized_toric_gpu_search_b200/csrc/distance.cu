@@ -880,18 +880,21 @@ int run_prepare(const DistArgs& args, cudaStream_t s) {
   return TG_OK;
 }
 
-int run_walk(const DistArgs& args, int sm_count, int blocks_per_sm, int tpb, cudaStream_t s) {
+int run_walk(const DistArgs& args, int sm_count, int blocks_per_sm, int tpb, cudaStream_t s,
+             int parts) {
   if (args.n <= 0) return TG_OK;
   const bool sampled = args.sample_count > 0;
   const int grid = sm_count * blocks_per_sm;
-  cudaError_t e;
-  switch (tpb) {
-    case 64: e = launch_walk<64>(args.variant, sampled, grid, blocks_per_sm, args, s); break;
-    case 256: e = launch_walk<256>(args.variant, sampled, grid, blocks_per_sm, args, s); break;
-    default: e = launch_walk<128>(args.variant, sampled, grid, blocks_per_sm, args, s); break;
+  cudaError_t e = cudaSuccess;
+  if (parts & kWalkEnumeration) {
+    switch (tpb) {
+      case 64: e = launch_walk<64>(args.variant, sampled, grid, blocks_per_sm, args, s); break;
+      case 256: e = launch_walk<256>(args.variant, sampled, grid, blocks_per_sm, args, s); break;
+      default: e = launch_walk<128>(args.variant, sampled, grid, blocks_per_sm, args, s); break;
+    }
   }
   if (e != cudaSuccess) return cuda_fail(e, "walk kernel launch");
-  if (args.is_min_k <= args.k_max) {
+  if ((parts & kWalkInfoset) && args.is_min_k <= args.k_max) {
     // Information-set walk: 512 resident threads per SM (128 registers).
     walk_infoset_kernel<kIsWalkThreads, 512 / kIsWalkThreads>
         <<<sm_count * (512 / kIsWalkThreads), kIsWalkThreads, 0, s>>>(args);

@@ -83,6 +83,11 @@ int default_tail_rows(const tg_distance_params& p);
 int infoset_min_k(const tg_distance_params& p);
 WsLayout ws_layout(const tg_distance_params& p);
 int run_prepare(const DistArgs& args, cudaStream_t s);
-int run_walk(const DistArgs& args, int sm_count, int blocks_per_sm, int tpb, cudaStream_t s);
+// parts: kWalkEnumeration (orbit / projective / sampled walk) and/or
+// kWalkInfoset (information-set walk and its finalisation).
+constexpr int kWalkEnumeration = 1;
+constexpr int kWalkInfoset = 2;
+int run_walk(const DistArgs& args, int sm_count, int blocks_per_sm, int tpb, cudaStream_t s,
+             int parts = kWalkEnumeration | kWalkInfoset);
 
 }  // namespace tg

@@ -501,7 +501,7 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) walk_infoset_kernel(DistArgs
   }
   // codewords evaluated, one atomic per warp
   for (int o = 16; o > 0; o >>= 1) evaluated += __shfl_xor_sync(0xffffffffu, evaluated, o);
-  if (lane == 0 && evaluated) atomicAdd(&a.hdr->codewords, evaluated);
+  if (lane == 0 && evaluated) atomicAdd(&a.is_hdr->codewords, evaluated);
 }
 
 __global__ void finalize_infoset_kernel(DistArgs a) {

@@ -156,13 +156,16 @@ class DistanceRunner:
 
     def walk(self, p: _lib.DistanceParams, d_out: torch.Tensor,
              stream: torch.cuda.Stream | None = None,
-             workspace: torch.Tensor | None = None) -> None:
+             workspace: torch.Tensor | None = None,
+             parts: int = _lib.TG_WALK_ENUMERATION | _lib.TG_WALK_INFOSET) -> None:
+        """Enqueues the walks (`parts`: a mask of TG_WALK_* values)."""
         ws = workspace if workspace is not None else self.workspace(p)
         st = stream if stream is not None else torch.cuda.current_stream(self.device)
         _lib.check(
-            _lib.load().tg_max_zeros_walk(self.ctx.handle, ctypes.byref(p), d_out.data_ptr(),
-                                          ws.data_ptr(), ws.numel(), st.cuda_stream),
-            "tg_max_zeros_walk",
+            _lib.load().tg_max_zeros_walk_part(self.ctx.handle, ctypes.byref(p), parts,
+                                               d_out.data_ptr(), ws.data_ptr(), ws.numel(),
+                                               st.cuda_stream),
+            "tg_max_zeros_walk_part",
         )
 
     def status(self, p: _lib.DistanceParams, stream: torch.cuda.Stream) -> int:
@@ -182,6 +185,16 @@ class DistanceRunner:
                                                     ctypes.byref(r)),
                    "tg_distance_counters")
         return int(t.value), int(c.value), float(r.value)
+
+    def path_counters(self, stream: torch.cuda.Stream | None = None) -> dict[str, int]:
+        """Tasks and codewords of the last run, per walk."""
+        st = stream if stream is not None else torch.cuda.current_stream(self.device)
+        h = (ctypes.c_uint64 * 4)()
+        _lib.check(_lib.load().tg_distance_path_counters(ctypes.byref(self.last_params),
+                                                         self._ws.data_ptr(), st.cuda_stream, h),
+                   "tg_distance_path_counters")
+        return {"enumeration_tasks": int(h[0]), "enumeration_codewords": int(h[1]),
+                "infoset_tasks_queued": int(h[2]), "infoset_codewords": int(h[3])}
 
 
 class DistanceOracleCUDABP:

@@ -144,10 +144,11 @@ int tg_max_zeros(tg_context* ctx, const tg_distance_params* p,
 
 /* The two halves of tg_max_zeros, for callers that time or capture them
  * separately: _prepare validates the sets, orders rows, builds the bit-sliced
- * bases and the task table (prep + scan kernels); _walk runs the persistent
- * enumeration kernel over the prepared tasks and writes d_out.  Same
- * arguments and workspace as tg_max_zeros; d_out of _prepare receives the
- * values of sets decided without enumeration (k <= 1, repeated rows). */
+ * bases, the information sets and the task tables (prep + scan kernels);
+ * _walk runs the persistent enumeration kernels over the prepared tasks and
+ * writes d_out.  Same arguments and workspace as tg_max_zeros; d_out of
+ * _prepare receives the values of sets decided without enumeration (k <= 1,
+ * dependent rows). */
 int tg_max_zeros_prepare(tg_context* ctx, const tg_distance_params* p,
                          const int32_t* d_indices, const int64_t* d_offsets,
                          const int32_t* d_target, const int32_t* d_set_ids,
@@ -156,6 +157,16 @@ int tg_max_zeros_prepare(tg_context* ctx, const tg_distance_params* p,
 int tg_max_zeros_walk(tg_context* ctx, const tg_distance_params* p,
                       int32_t* d_out, void* d_workspace, size_t workspace_bytes,
                       void* stream);
+
+/* One part of tg_max_zeros_walk, for callers that time the two walks apart:
+ * TG_WALK_ENUMERATION runs the orbit / projective / sampled walk (sets below
+ * the information-set threshold), TG_WALK_INFOSET the information-set walk
+ * and the step that writes its results.  tg_max_zeros_walk is both, in that
+ * order; the parts touch disjoint sets, so either order gives the same d_out. */
+enum { TG_WALK_ENUMERATION = 1, TG_WALK_INFOSET = 2 };
+int tg_max_zeros_walk_part(tg_context* ctx, const tg_distance_params* p,
+                           int32_t parts, int32_t* d_out, void* d_workspace,
+                           size_t workspace_bytes, void* stream);
 
 /* Size of the library-owned scratch area tg_max_zeros_noalloc works in. */
 #define TG_STATIC_WORKSPACE_BYTES (16u << 20)
@@ -193,6 +204,13 @@ int tg_distance_status(const tg_distance_params* p, const void* d_workspace,
 int tg_distance_counters(const tg_distance_params* p, const void* d_workspace,
                          void* stream, uint64_t* h_tasks,
                          uint64_t* h_codewords, double* h_reference_messages);
+
+/* The same accounting per walk (synchronises `stream`): h_counts[0..3] =
+ * enumeration walk tasks and codewords, information-set tasks queued (every
+ * level of every set, most of them skipped once a set is finished) and
+ * codewords the information-set walk evaluated. */
+int tg_distance_path_counters(const tg_distance_params* p, const void* d_workspace,
+                              void* stream, uint64_t* h_counts);
 
 /* ---- canonical forms ---------------------------------------------------- */
 
