@@ -107,10 +107,7 @@ int infoset_min_k(const tg_distance_params& p) {
 // Rows (sets x k) an information-set code of k_lo <= k <= k_hi may store.
 static int infoset_rows(int k_lo, int k_hi) {
   int rows = 0;
-  for (int k = k_lo; k <= k_hi; ++k) {
-    const int sets = std::min(8, 64 / k);  // kIsMaxSets, kIsMaxRows
-    rows = std::max(rows, sets * k);
-  }
+  for (int k = k_lo; k <= k_hi; ++k) rows = std::max(rows, infoset_max_sets(k) * k);
   return rows;
 }
 
@@ -136,7 +133,7 @@ WsLayout ws_layout(const tg_distance_params& p) {
   L.is_min_k = infoset_min_k(p);
   const bool infoset = L.is_min_k <= kmax;
   const size_t levels = infoset ? n * size_t(kmax) : 0;
-  L.is_stride = infoset ? infoset_rows(L.is_min_k, kmax) * 7 : 0;  // kIsVecPerRow
+  L.is_stride = infoset ? infoset_rows(L.is_min_k, kmax) * kIsVecPerRow : 0;
   L.is_hdr = off;   off = align256(off + (infoset ? sizeof(WsHeader) : 0));
   L.is_rows = off;  off = align256(off + n * size_t(L.is_stride) * sizeof(V6));
   L.is_cnt = off;   off = align256(off + levels * sizeof(uint64_t));

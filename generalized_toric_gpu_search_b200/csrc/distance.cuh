@@ -33,6 +33,21 @@ struct CodeDesc {
 constexpr int32_t kDecidedFlag = 1;  // value known after preparation
 constexpr int32_t kIsCodeFlag = 2;   // evaluated by information sets
 
+constexpr int kIsMaxSets = 8;     // information sets per code
+constexpr int kIsMaxRows = 64;    // sets x k per code
+constexpr int kIsVecPerRow = 7;   // g and the deltas (alpha^v + alpha^(v+1)) g, v = 0..5
+constexpr int kIsMaxDelta = 3;    // a partial set is kept when k - rank <= this
+
+// Most information sets a code of k rows stores: the full ones that fit in
+// 49 columns, plus a partial one when the leftover columns could give it a
+// rank deficit <= kIsMaxDelta, within kIsMaxSets and kIsMaxRows.
+__host__ __device__ constexpr int infoset_max_sets(int k) {
+  const int cap = kIsMaxSets < kIsMaxRows / k ? kIsMaxSets : kIsMaxRows / k;
+  const int full = cap < 49 / k ? cap : 49 / k;
+  const int partial = (full < cap && 49 - full * k >= k - kIsMaxDelta && 49 - full * k > 0) ? 1 : 0;
+  return full + partial;
+}
+
 struct WsLayout {
   size_t hdr, desc, task_off, abort, basis, pat_cum, pat_info, bitpat;
   size_t is_hdr, is_rows, is_cnt, is_off, is_done, is_best, is_bits, total;

@@ -37,11 +37,7 @@
 namespace tg {
 
 constexpr int kIsInner = 5;       // Gray-walked coefficients per task (7^5 codewords)
-constexpr int kIsMaxSets = 8;     // information sets per code
-constexpr int kIsMaxRows = 64;    // sets x k per code
-constexpr int kIsVecPerRow = 7;   // g and the deltas (alpha^v + alpha^(v+1)) g, v = 0..5
 constexpr int kIsTries = 32;      // column orders tried per code
-constexpr int kIsMaxDelta = 3;    // a partial set is kept when k - rank <= this
 constexpr int kIsBinom = 22;      // binomial table side (n, r <= 21)
 
 // ---------------------------------------------------------------------------
