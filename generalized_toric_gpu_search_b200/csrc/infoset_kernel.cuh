@@ -155,9 +155,33 @@ __device__ __forceinline__ void is_store_set(V6* dst, int lane, int k, uint64_t 
   }
 }
 
+// Shape of the level-w tasks of one set, n_supports = C(k, w).  Every task
+// covers about 7^kIsInner codewords: below level kIsInner + 1 a task walks
+// `group` consecutive supports completely; from there on a task is one
+// support and one block of the outer coefficients (group = 1).
+struct IsTaskShape {
+  int inner;                     // Gray-walked coefficients per support
+  int outer;                     // coefficients fixed by the task's block
+  unsigned long long group;      // supports per task
+  unsigned long long per_set;    // tasks per set
+};
+
+__device__ __forceinline__ IsTaskShape is_task_shape(unsigned long long n_supports, int w) {
+  IsTaskShape s;
+  s.inner = min(w - 1, kIsInner);
+  s.outer = w - 1 - s.inner;
+  if (s.outer > 0) {
+    s.group = 1ull;
+    s.per_set = n_supports * c_pow7[s.outer];
+  } else {
+    s.group = c_pow7[kIsInner - s.inner];
+    s.per_set = (n_supports + s.group - 1ull) / s.group;
+  }
+  return s;
+}
+
 __device__ __forceinline__ unsigned long long is_tasks_per_set(int k, int w) {
-  const int outer = max(0, w - 1 - kIsInner);
-  return c_binom[k][w] * c_pow7[outer];
+  return is_task_shape(c_binom[k][w], w).per_set;
 }
 
 __global__ void __launch_bounds__(kIsPrepWarps * 32) prep_infoset_kernel(DistArgs a) {
@@ -346,97 +370,155 @@ __device__ __forceinline__ void v6_alpha(V6& p) {
   p.h0 = t;
 }
 
-// One task: the smallest weight met and the codewords evaluated.
+// Delta of the move between 49-codeword blocks b - 1 and b (b >= 1): digit
+// 2 + tz moves, tz = trailing base-7 zeros of b.  It runs up when the digits
+// above it sum to an even number, between alpha^v and alpha^(v+1).
+__device__ __forceinline__ const V6* is_block_move(const V6* rows, unsigned b, uint32_t r2,
+                                                  uint32_t r3, uint32_t r4) {
+  unsigned q = b;
+  int tz = 0;
+  while (q % 7u == 0u) {
+    q /= 7u;
+    ++tz;
+  }
+  const unsigned ot = q % 7u;
+  const int v = ((q / 7u) & 1u) ? int(6u - ot) : int(ot - 1u);
+  const uint32_t R = tz == 0 ? r2 : (tz == 1 ? r3 : r4);
+  return rows + R + 1 + v;
+}
+
+#define TG_IS_STEP(D) \
+  v6_xor(cw, D);      \
+  is_weight(cw, wmin)
+#define TG_IS_SWEEP_UP \
+  TG_IS_STEP(d0); TG_IS_STEP(d1); TG_IS_STEP(d2); TG_IS_STEP(d3); TG_IS_STEP(d4); TG_IS_STEP(d5)
+#define TG_IS_SWEEP_DOWN \
+  TG_IS_STEP(d5); TG_IS_STEP(d4); TG_IS_STEP(d3); TG_IS_STEP(d2); TG_IS_STEP(d1); TG_IS_STEP(d0)
+
+// Walks the 7^inner codewords of one support from cw (every walked
+// coefficient alpha^0).  Digit 0 (row r0) and digit 1 (row r1) keep their six
+// deltas in registers, so the walk is straight-line code over blocks of 49
+// codewords; the one move between blocks (digits 2..4, rows r2..r4) is loaded
+// a block ahead.  Rows are vector offsets from `rows`.  Returns the codewords
+// evaluated.
+__device__ __forceinline__ unsigned long long is_walk_support(V6 cw, int inner, const V6* rows,
+                                                              uint32_t r0, uint32_t r1,
+                                                              uint32_t r2, uint32_t r3,
+                                                              uint32_t r4, int wthr,
+                                                              const int32_t* stop, int& wmin) {
+  is_weight(cw, wmin);
+  if (inner == 0) return 1ull;
+  const V6* R0 = rows + r0;
+  const V6 d0 = v6_ldg(R0 + 1), d1 = v6_ldg(R0 + 2), d2 = v6_ldg(R0 + 3);
+  const V6 d3 = v6_ldg(R0 + 4), d4 = v6_ldg(R0 + 5), d5 = v6_ldg(R0 + 6);
+  if (inner == 1) {
+    TG_IS_SWEEP_UP;
+    return 7ull;
+  }
+  const V6* R1 = rows + r1;
+  const V6 e0 = v6_ldg(R1 + 1), e1 = v6_ldg(R1 + 2), e2 = v6_ldg(R1 + 3);
+  const V6 e3 = v6_ldg(R1 + 4), e4 = v6_ldg(R1 + 5), e5 = v6_ldg(R1 + 6);
+  const unsigned blocks = static_cast<unsigned>(c_pow7[inner - 2]);
+  V6 nx;
+  v6_zero(nx);
+  if (blocks > 1u) nx = v6_ldg(is_block_move(rows, 1u, r2, r3, r4));
+  unsigned b = 0;
+  for (; b < blocks; ++b) {
+    if (b) {
+      TG_IS_STEP(nx);
+      if (b + 1u < blocks) nx = v6_ldg(is_block_move(rows, b + 1u, r2, r3, r4));
+    }
+    // Digit 0 runs up in sweep s of block b when b + s is even; digit 1 runs
+    // up through the block when b is even.
+    if ((b & 1u) == 0u) {
+      TG_IS_SWEEP_UP;   TG_IS_STEP(e0);
+      TG_IS_SWEEP_DOWN; TG_IS_STEP(e1);
+      TG_IS_SWEEP_UP;   TG_IS_STEP(e2);
+      TG_IS_SWEEP_DOWN; TG_IS_STEP(e3);
+      TG_IS_SWEEP_UP;   TG_IS_STEP(e4);
+      TG_IS_SWEEP_DOWN; TG_IS_STEP(e5);
+      TG_IS_SWEEP_UP;
+    } else {
+      TG_IS_SWEEP_DOWN; TG_IS_STEP(e5);
+      TG_IS_SWEEP_UP;   TG_IS_STEP(e4);
+      TG_IS_SWEEP_DOWN; TG_IS_STEP(e3);
+      TG_IS_SWEEP_UP;   TG_IS_STEP(e2);
+      TG_IS_SWEEP_DOWN; TG_IS_STEP(e1);
+      TG_IS_SWEEP_UP;   TG_IS_STEP(e0);
+      TG_IS_SWEEP_DOWN;
+    }
+    if (wmin < wthr) break;
+    if ((b & 15u) == 15u && ld_flag(stop)) break;
+  }
+  return 49ull * (min(b, blocks - 1u) + 1u);
+}
+
+#undef TG_IS_SWEEP_DOWN
+#undef TG_IS_SWEEP_UP
+#undef TG_IS_STEP
+
+// One task: its supports walked completely; the smallest weight met, and the
+// codewords evaluated in ncw.
 __device__ __forceinline__ int is_task(const DistArgs& a,
                                        const unsigned long long (*bn)[kIsBinom], int c, int k,
                                        int w, unsigned long long local, int wthr,
                                        unsigned long long& ncw) {
-  const int inner = min(w - 1, kIsInner);
-  const int outer = w - 1 - inner;
-  const unsigned long long B = c_pow7[outer];
-  const unsigned long long per_set = bn[k][w] * B;
-  const int j = int(local / per_set);
-  const unsigned long long rr = local - static_cast<unsigned long long>(j) * per_set;
-  unsigned long long srank = rr / B;
-  unsigned long long blk = rr - srank * B;
+  const unsigned long long n_sup = bn[k][w];
+  const IsTaskShape sh = is_task_shape(n_sup, w);
+  const int j = int(local / sh.per_set);
+  const unsigned long long rr = local - static_cast<unsigned long long>(j) * sh.per_set;
+  const unsigned long long B = c_pow7[sh.outer];
+  // supports [s_beg, s_end) of C(k, w) <= C(21, 10) fit 32 bits
+  uint32_t s_beg, s_end;
+  unsigned long long blk0;
+  if (sh.outer > 0) {
+    s_beg = uint32_t(rr / B);
+    s_end = s_beg + 1u;
+    blk0 = rr - static_cast<unsigned long long>(s_beg) * B;
+  } else {
+    s_beg = uint32_t(rr * sh.group);
+    s_end = uint32_t(min(rr * sh.group + sh.group, n_sup));
+    blk0 = 0ull;
+  }
   const V6* rows = a.is_rows + size_t(c) * a.is_stride + size_t(j) * k * kIsVecPerRow;
-  // Support rows from the largest down (combinadic unranking).  The q-th row
-  // found is inner digit q while q < inner, then the outer rows from the top
-  // block digit down, and last the row with coefficient 1.
-  V6 cw;
-  v6_zero(cw);
-  const V6 *r0 = rows, *r1 = rows, *r2 = rows, *r3 = rows, *r4 = rows;
-  unsigned long long P = outer > 0 ? c_pow7[outer - 1] : 1ull;
-  int rem = w, q = 0;
-  for (int pos = k - 1; pos >= 0 && rem > 0; --pos) {
-    const unsigned long long b = bn[pos][rem];
-    if (srank < b) continue;
-    srank -= b;
-    --rem;
-    const V6* R = rows + pos * kIsVecPerRow;
-    V6 g = v6_ldg(R);
-    if (q < inner) {
-      if (q == 0) r0 = R;
-      else if (q == 1) r1 = R;
-      else if (q == 2) r2 = R;
-      else if (q == 3) r3 = R;
-      else r4 = R;
-    } else if (rem > 0) {
-      const unsigned long long e = blk / P;
-      blk -= e * P;
-      P /= 7ull;
-      for (unsigned long long i = 0; i < e; ++i) v6_alpha(g);
-    }
-    v6_xor(cw, g);
-    ++q;
-  }
-  int wmin = 64;
-  is_weight(cw, wmin);
-  if (inner == 0) {
-    ncw = 1ull;
-    return wmin;
-  }
-  const V6 d0 = v6_ldg(r0 + 1), d1 = v6_ldg(r0 + 2), d2 = v6_ldg(r0 + 3);
-  const V6 d3 = v6_ldg(r0 + 4), d4 = v6_ldg(r0 + 5), d5 = v6_ldg(r0 + 6);
-  const unsigned sweeps = static_cast<unsigned>(c_pow7[inner - 1]);
   const int32_t* stop = a.abort + c;
-  unsigned o = 0;
-  for (; o < sweeps; ++o) {
-    if (o) {
-      // Digit 1 + tz moves, tz = trailing base-7 zeros of o.  It runs up when
-      // the digits above it sum to an even number, and moves between
-      // alpha^v and alpha^(v+1).
-      unsigned qq = o;
-      int tz = 0;
-      while (qq % 7u == 0u) {
-        qq /= 7u;
-        ++tz;
+  int wmin = 64;
+  ncw = 0ull;
+  for (uint32_t s = s_beg; s < s_end; ++s) {
+    // Support rows from the largest down (combinadic unranking).  The q-th
+    // row found is inner digit q while q < inner, then the outer rows from the
+    // top block digit down, and last the row with coefficient 1.
+    V6 cw;
+    v6_zero(cw);
+    uint32_t r0 = 0u, r1 = 0u, r2 = 0u, r3 = 0u, r4 = 0u;
+    unsigned long long srank = s, blk = blk0;
+    unsigned long long P = sh.outer > 0 ? c_pow7[sh.outer - 1] : 1ull;
+    int rem = w, q = 0;
+    for (int pos = k - 1; pos >= 0 && rem > 0; --pos) {
+      const unsigned long long b = bn[pos][rem];
+      if (srank < b) continue;
+      srank -= b;
+      --rem;
+      const uint32_t R = uint32_t(pos * kIsVecPerRow);
+      V6 g = v6_ldg(rows + R);
+      if (q < sh.inner) {
+        if (q == 0) r0 = R;
+        else if (q == 1) r1 = R;
+        else if (q == 2) r2 = R;
+        else if (q == 3) r3 = R;
+        else r4 = R;
+      } else if (rem > 0) {
+        const unsigned long long e = blk / P;
+        blk -= e * P;
+        P /= 7ull;
+        for (unsigned long long i = 0; i < e; ++i) v6_alpha(g);
       }
-      const unsigned ot = qq % 7u;
-      const int v = ((qq / 7u) & 1u) ? int(6u - ot) : int(ot - 1u);
-      const V6* R = tz == 0 ? r1 : (tz == 1 ? r2 : (tz == 2 ? r3 : r4));
-      v6_xor(cw, v6_ldg(R + 1 + v));
-      is_weight(cw, wmin);
+      v6_xor(cw, g);
+      ++q;
     }
-    if ((o & 1u) == 0u) {
-      v6_xor(cw, d0); is_weight(cw, wmin);
-      v6_xor(cw, d1); is_weight(cw, wmin);
-      v6_xor(cw, d2); is_weight(cw, wmin);
-      v6_xor(cw, d3); is_weight(cw, wmin);
-      v6_xor(cw, d4); is_weight(cw, wmin);
-      v6_xor(cw, d5); is_weight(cw, wmin);
-    } else {
-      v6_xor(cw, d5); is_weight(cw, wmin);
-      v6_xor(cw, d4); is_weight(cw, wmin);
-      v6_xor(cw, d3); is_weight(cw, wmin);
-      v6_xor(cw, d2); is_weight(cw, wmin);
-      v6_xor(cw, d1); is_weight(cw, wmin);
-      v6_xor(cw, d0); is_weight(cw, wmin);
-    }
+    ncw += is_walk_support(cw, sh.inner, rows, r0, r1, r2, r3, r4, wthr, stop, wmin);
     if (wmin < wthr) break;
-    if ((o & 63u) == 63u && ld_flag(stop)) break;
   }
-  ncw = 7ull * (min(o, sweeps - 1u) + 1u);
   return wmin;
 }
 
@@ -474,10 +556,9 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) walk_infoset_kernel(DistArgs
       atomicMax(&a.is_hdr->counter, r_end);
       continue;
     }
-    const CodeDesc d = a.desc[c];
-    const int wthr = kN - d.tmax;
+    const int wthr = kN - a.desc[c].tmax;
     unsigned long long ncw = 0ull;
-    const int wmin = is_task(a, s_binom, c, d.k, w, t - r_beg, wthr, ncw);
+    const int wmin = is_task(a, s_binom, c, a.desc[c].k, w, t - r_beg, wthr, ncw);
     evaluated += ncw;
     const int best = min(atomicMin(a.is_best + c, wmin), wmin);
     if (best < wthr) {
@@ -491,6 +572,7 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) walk_infoset_kernel(DistArgs
       const unsigned bits = atomicOr(a.is_bits + c, bit) | bit;
       const int L = __ffs(~bits) - 1;
       const int now = atomicAdd(a.is_best + c, 0);
+      const CodeDesc d = a.desc[c];
       const int bound = d.R * (L + 1) + (d.n_pat > 0 ? max(0, L + 1 - d.n_pat) : 0);
       if (L >= d.k || now <= bound) is_finish(a, c, r_end);
     }
