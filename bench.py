@@ -41,9 +41,12 @@ UNIT = "codewords/s"
 WORKLOAD = "batched uneven evaluation: 10,000 seeded random P, |P|~U{6..14}, td=1, exact"
 POPC_PER_CODEWORD = 14.0 / 8.0  # histogram walk: 7 bins x 2 words per 8 codewords
 POPC_PER_CODEWORD_INFOSET = 2.0  # information-set walk: one weight per codeword
-# Kernels per step: prep_exact, prep_infoset, scan_levels, scan_tasks,
-# walk_hist, walk_infoset, finalize_infoset.
-LAUNCHES_PER_STEP = 7
+
+
+def launches_per_step(k_max: int) -> int:
+    """Kernels per step: prep_exact, prep_infoset, scan_tasks, walk_hist, then
+    per information-set level plan, scan and walk, and finalize_infoset."""
+    return 5 + 3 * k_max
 L2_FLUSH_BYTES = 256 << 20
 
 
@@ -613,7 +616,7 @@ def run_b200_arm(args, d: Dist) -> None:
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * e2e_max / args.steps,
                     "api": "DistanceOracleCUDABP.max_zeros_batch(list of lists, 1)"},
-            "gpu_launches": LAUNCHES_PER_STEP * args.steps,
+            "gpu_launches": launches_per_step(kmax) * args.steps,
             "roofline": {"bound": "int (POPC pipe)", "achieved": achieved / 1e12,
                          "peak": peak / 1e12, "unit": "Tpopc/s", "frac": achieved / peak,
                          "traffic": None, "kernel": dominant["kernel"],

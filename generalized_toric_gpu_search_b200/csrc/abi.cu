@@ -248,13 +248,11 @@ static void bind_workspace(DistArgs& a, const WsLayout& L, void* ws) {
   a.bitpat_stride = L.bitpat_stride;
   a.is_min_k = L.is_min_k;
   a.is_stride = L.is_stride;
-  a.is_hdr = reinterpret_cast<WsHeader*>(b + L.is_hdr);
+  a.is_hdr = reinterpret_cast<IsHeader*>(b + L.is_hdr);
   a.is_rows = reinterpret_cast<V6*>(b + L.is_rows);
-  a.is_cnt = reinterpret_cast<uint64_t*>(b + L.is_cnt);
+  a.is_units = reinterpret_cast<uint64_t*>(b + L.is_units);
   a.is_off = reinterpret_cast<uint64_t*>(b + L.is_off);
-  a.is_done = reinterpret_cast<unsigned long long*>(b + L.is_done);
   a.is_best = reinterpret_cast<int32_t*>(b + L.is_best);
-  a.is_bits = reinterpret_cast<uint32_t*>(b + L.is_bits);
 }
 
 // Validates a max_zeros call and fills the kernel arguments.
@@ -391,13 +389,13 @@ int tg_distance_counters(const tg_distance_params* p, const void* d_workspace, v
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   cudaError_t e = cudaMemcpyAsync(&h, static_cast<const uint8_t*>(d_workspace) + L.hdr, sizeof(h),
                                   cudaMemcpyDeviceToHost, s);
-  WsHeader hi{};
+  IsHeader hi{};
   if (e == cudaSuccess && L.is_min_k <= p->k_max && p->n_sets > 0)
     e = cudaMemcpyAsync(&hi, static_cast<const uint8_t*>(d_workspace) + L.is_hdr, sizeof(hi),
                         cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_fail(e, "tg_distance_counters");
-  if (h_tasks) *h_tasks = h.total_tasks + hi.total_tasks;
+  if (h_tasks) *h_tasks = h.total_tasks + hi.tasks_all;
   if (h_codewords) *h_codewords = h.codewords + hi.codewords;
   if (h_reference_messages) *h_reference_messages = h.ref_messages;
   return TG_OK;
@@ -409,7 +407,8 @@ int tg_distance_path_counters(const tg_distance_params* p, const void* d_workspa
   if (st) return st;
   if (!d_workspace || !h_counts) return invalid("tg_distance_path_counters: NULL argument");
   const WsLayout L = ws_layout(*p);
-  WsHeader h{}, hi{};
+  WsHeader h{};
+  IsHeader hi{};
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const uint8_t* b = static_cast<const uint8_t*>(d_workspace);
   cudaError_t e = cudaMemcpyAsync(&h, b + L.hdr, sizeof(h), cudaMemcpyDeviceToHost, s);
@@ -419,7 +418,7 @@ int tg_distance_path_counters(const tg_distance_params* p, const void* d_workspa
   if (e != cudaSuccess) return cuda_fail(e, "tg_distance_path_counters");
   h_counts[0] = h.total_tasks;
   h_counts[1] = h.codewords;
-  h_counts[2] = hi.total_tasks;
+  h_counts[2] = hi.tasks_all;
   h_counts[3] = hi.codewords;
   return TG_OK;
 }

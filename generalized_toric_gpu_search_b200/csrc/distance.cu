@@ -132,15 +132,13 @@ WsLayout ws_layout(const tg_distance_params& p) {
   L.bitpat = off;   off = align256(off + n * size_t(L.bitpat_stride) * sizeof(V6));
   L.is_min_k = infoset_min_k(p);
   const bool infoset = L.is_min_k <= kmax;
-  const size_t levels = infoset ? n * size_t(kmax) : 0;
+  const size_t n_is = infoset ? n : 0;
   L.is_stride = infoset ? infoset_rows(L.is_min_k, kmax) * kIsVecPerRow : 0;
-  L.is_hdr = off;   off = align256(off + (infoset ? sizeof(WsHeader) : 0));
+  L.is_hdr = off;   off = align256(off + (infoset ? sizeof(IsHeader) : 0));
   L.is_rows = off;  off = align256(off + n * size_t(L.is_stride) * sizeof(V6));
-  L.is_cnt = off;   off = align256(off + levels * sizeof(uint64_t));
-  L.is_off = off;   off = align256(off + (infoset ? levels + 1 : 0) * sizeof(uint64_t));
-  L.is_done = off;  off = align256(off + levels * sizeof(uint64_t));
-  L.is_best = off;  off = align256(off + (infoset ? n : 0) * sizeof(int32_t));
-  L.is_bits = off;  off = align256(off + (infoset ? n : 0) * sizeof(uint32_t));
+  L.is_units = off; off = align256(off + n_is * sizeof(uint64_t));
+  L.is_off = off;   off = align256(off + (infoset ? n + 1 : 0) * sizeof(uint64_t));
+  L.is_best = off;  off = align256(off + n_is * sizeof(int32_t));
   L.total = off;
   return L;
 }
@@ -863,11 +861,10 @@ int run_prepare(const DistArgs& args, cudaStream_t s) {
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "prep kernel launch");
   if (args.is_min_k <= args.k_max) {
-    e = cudaMemsetAsync(args.is_hdr, 0, sizeof(WsHeader), s);
+    e = cudaMemsetAsync(args.is_hdr, 0, sizeof(IsHeader), s);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(information-set header)");
     prep_infoset_kernel<<<(args.n + kIsPrepWarps - 1) / kIsPrepWarps, kIsPrepWarps * 32, 0, s>>>(
         args);
-    scan_levels_kernel<<<1, kScanThreads, 0, s>>>(args);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "information-set prep launch");
   }
@@ -892,10 +889,18 @@ int run_walk(const DistArgs& args, int sm_count, int blocks_per_sm, int tpb, cud
   }
   if (e != cudaSuccess) return cuda_fail(e, "walk kernel launch");
   if ((parts & kWalkInfoset) && args.is_min_k <= args.k_max) {
-    // Information-set walk: 512 resident threads per SM (128 registers).
-    walk_infoset_kernel<kIsWalkThreads, 512 / kIsWalkThreads>
-        <<<sm_count * (512 / kIsWalkThreads), kIsWalkThreads, 0, s>>>(args);
-    finalize_infoset_kernel<<<(args.n + 255) / 256, 256, 0, s>>>(args);
+    // Information-set walk, one level per launch triple; 512 resident
+    // threads per SM (128 registers).  Levels no code needs find no tasks.
+    constexpr int kPerSm = 512 / kIsWalkThreads;
+    DistArgs la = args;
+    la.is_lanes = sm_count * 512;
+    const int plan_grid = (args.n + 255) / 256;
+    for (int w = 1; w <= args.k_max; ++w) {
+      plan_level_kernel<<<plan_grid, 256, 0, s>>>(la, w);
+      scan_level_kernel<<<1, kScanThreads, 0, s>>>(la, w);
+      walk_level_kernel<kIsWalkThreads, kPerSm><<<sm_count * kPerSm, kIsWalkThreads, 0, s>>>(la, w);
+    }
+    finalize_infoset_kernel<<<plan_grid, 256, 0, s>>>(la);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "information-set walk launch");
   }

@@ -15,6 +15,17 @@ struct WsHeader {
   double ref_messages;            // sum over exact sets of 8^k - 1
 };
 
+// Header of the information-set walk (one level at a time).
+struct IsHeader {
+  unsigned long long counter;    // next unclaimed task of the level being walked
+  unsigned long long total;      // tasks of that level
+  unsigned long long units;      // units (49-codeword blocks) per task of that level
+  unsigned long long tasks_all;  // tasks over all levels walked
+  unsigned long long codewords;  // codewords evaluated
+  int32_t level;
+  int32_t pad;
+};
+
 // Per-code descriptor written by the prep kernels.
 struct CodeDesc {
   int32_t k;        // rows of the code
@@ -50,7 +61,7 @@ __host__ __device__ constexpr int infoset_max_sets(int k) {
 
 struct WsLayout {
   size_t hdr, desc, task_off, abort, basis, pat_cum, pat_info, bitpat;
-  size_t is_hdr, is_rows, is_cnt, is_off, is_done, is_best, is_bits, total;
+  size_t is_hdr, is_rows, is_units, is_off, is_best, total;
   int basis_stride, pat_stride, bitpat_stride, is_stride, is_min_k;
 };
 
@@ -82,13 +93,12 @@ struct DistArgs {
   // Information-set path: codes with is_min_k <= k (is_min_k > k_max: none).
   int is_min_k;
   int is_stride;                 // V6 per code in is_rows
-  WsHeader* is_hdr;              // task queue of the information-set walk
+  int is_lanes;                  // resident threads of the walk (task sizing)
+  IsHeader* is_hdr;              // task queue of the information-set walk
   V6* is_rows;                   // per code and set: k rows x (g, 6 deltas)
-  uint64_t* is_cnt;              // tasks per (level, code), level-major
-  uint64_t* is_off;              // exclusive scan of is_cnt (n * k_max + 1)
-  unsigned long long* is_done;   // finished tasks per (level, code)
+  uint64_t* is_units;            // units of the current level per code
+  uint64_t* is_off;              // task offsets of the current level (n + 1)
   int32_t* is_best;              // smallest weight met per code
-  uint32_t* is_bits;             // completed levels per code (bit w - 1)
   DeviceTables tab;
 };
 

@@ -23,20 +23,25 @@
 // partial rank.  One lane holds one row, bit-sliced over the 49 columns, so a
 // pivot step is a ballot, a row swap and one broadcast.
 //
-// Tasks: (level w, code, set j, support T of w rows, block of outer
-// coefficients).  The first row of T has coefficient 1; the next
-// w - 1 - inner rows ("outer") take the block's base-7 digits as powers
-// alpha^e; the last inner = min(w - 1, 5) rows walk a reflected base-7 Gray
-// code over alpha^0..alpha^6, one XOR of a precomputed delta
-// (alpha^v + alpha^(v+1)) g per codeword.  The global queue is level-major
-// over the batch, so a code's level w + 1 starts after its level w has been
-// handed out, and a finished code's remaining range is skipped by moving the
-// counter past it.
+// Walk.  A support T of w rows has its first row at coefficient 1; the other
+// w - 1 rows walk a reflected base-7 Gray code over alpha^0..alpha^6, one XOR
+// of a precomputed delta (alpha^v + alpha^(v+1)) g per codeword.  The two
+// fastest digits form straight-line blocks of 49 codewords with their deltas
+// in registers; a task is a range of blocks (of one or more supports), and
+// can start at any block because the Gray position of a block start has a
+// closed form.
+//
+// Levels run one launch at a time: plan_level_kernel finishes the codes whose
+// bound is met and sizes the next level of the others, scan_level_kernel
+// picks the task size from the level's total work (about eight tasks per
+// resident thread, at most ~16807 codewords) and the offsets, and
+// walk_level_kernel hands the tasks to a persistent grid.  No code starts a
+// level before the previous one is complete, so no work is spent on levels a
+// code turns out not to need.
 #pragma once
 
 namespace tg {
 
-constexpr int kIsInner = 5;       // Gray-walked coefficients per task (7^5 codewords)
 constexpr int kIsTries = 32;      // column orders tried per code
 constexpr int kIsBinom = 22;      // binomial table side (n, r <= 21)
 
@@ -155,35 +160,6 @@ __device__ __forceinline__ void is_store_set(V6* dst, int lane, int k, uint64_t 
   }
 }
 
-// Shape of the level-w tasks of one set, n_supports = C(k, w).  Every task
-// covers about 7^kIsInner codewords: below level kIsInner + 1 a task walks
-// `group` consecutive supports completely; from there on a task is one
-// support and one block of the outer coefficients (group = 1).
-struct IsTaskShape {
-  int inner;                     // Gray-walked coefficients per support
-  int outer;                     // coefficients fixed by the task's block
-  unsigned long long group;      // supports per task
-  unsigned long long per_set;    // tasks per set
-};
-
-__device__ __forceinline__ IsTaskShape is_task_shape(unsigned long long n_supports, int w) {
-  IsTaskShape s;
-  s.inner = min(w - 1, kIsInner);
-  s.outer = w - 1 - s.inner;
-  if (s.outer > 0) {
-    s.group = 1ull;
-    s.per_set = n_supports * c_pow7[s.outer];
-  } else {
-    s.group = c_pow7[kIsInner - s.inner];
-    s.per_set = (n_supports + s.group - 1ull) / s.group;
-  }
-  return s;
-}
-
-__device__ __forceinline__ unsigned long long is_tasks_per_set(int k, int w) {
-  return is_task_shape(c_binom[k][w], w).per_set;
-}
-
 __global__ void __launch_bounds__(kIsPrepWarps * 32) prep_infoset_kernel(DistArgs a) {
   __shared__ uint8_t s_ord[kIsPrepWarps][64];
   const int wl = threadIdx.x >> 5;
@@ -197,13 +173,7 @@ __global__ void __launch_bounds__(kIsPrepWarps * 32) prep_infoset_kernel(DistArg
   int k = (klong >= a.is_min_k && klong <= a.k_max) ? int(klong) : 0;
   const int my = lane < k ? a.idx[beg + lane] : 0;
   if (__any_sync(0xffffffffu, lane < k && (my < 0 || my >= kN))) k = 0;
-  if (k == 0) {
-    for (int w = lane; w < a.k_max; w += 32) {
-      a.is_cnt[size_t(w) * a.n + c] = 0ull;
-      a.is_done[size_t(w) * a.n + c] = 0ull;
-    }
-    return;
-  }
+  if (k == 0) return;
   uint64_t o0 = 0ull, o1 = 0ull, o2 = 0ull;
   if (lane < k) {
     for (int j = 0; j < kN; ++j) {
@@ -260,12 +230,6 @@ __global__ void __launch_bounds__(kIsPrepWarps * 32) prep_infoset_kernel(DistArg
       ++m_full;
     }
   }
-  for (int w = 1 + lane; w <= a.k_max; w += 32) {
-    unsigned long long cnt = 0ull;
-    if (!deficient && w <= k) cnt = static_cast<unsigned long long>(n_sets) * is_tasks_per_set(k, w);
-    a.is_cnt[size_t(w - 1) * a.n + c] = cnt;
-    a.is_done[size_t(w - 1) * a.n + c] = 0ull;
-  }
   if (lane == 0) {
     CodeDesc d{};
     d.k = k;
@@ -280,77 +244,130 @@ __global__ void __launch_bounds__(kIsPrepWarps * 32) prep_infoset_kernel(DistArg
     a.out[c] = deficient ? kN : 0;
     a.abort[c] = deficient ? 1 : 0;
     a.is_best[c] = deficient ? 0 : 64;
-    a.is_bits[c] = 0u;
     atomicAdd(&a.hdr->ref_messages, double(pow8(k)) - 1.0);
   }
 }
 
-// Exclusive scan of the level-major task counts (one CTA of 1024 threads).
-__global__ void __launch_bounds__(kScanThreads) scan_levels_kernel(DistArgs a) {
+// ---------------------------------------------------------------------------
+// One level at a time: plan (which codes go on, how many units each), scan
+// (task size and offsets), walk.  Units are 49-codeword Gray blocks of one
+// support (whole supports of 1 or 7 codewords at levels 1 and 2).
+// ---------------------------------------------------------------------------
+
+// Units of one support at level w.
+__device__ __forceinline__ unsigned long long is_units_per_support(int w) {
+  return w >= 3 ? c_pow7[w - 3] : 1ull;
+}
+
+// Most units a task takes at level w (about 16807 codewords).
+__device__ __forceinline__ unsigned long long is_max_task_units(int w) {
+  return w >= 3 ? 343ull : (w == 2 ? 2401ull : 16807ull);
+}
+
+// Decides, with levels 1..w-1 complete, whether each code is finished, and
+// the units of level w of those that are not.
+__global__ void plan_level_kernel(DistArgs a, int w) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.n) return;
+  unsigned long long units = 0ull;
+  const CodeDesc d = a.desc[c];
+  if ((d.flags & kIsCodeFlag) != 0 && (d.flags & kDecidedFlag) == 0 && a.abort[c] == 0) {
+    const int best = a.is_best[c];
+    const int L = w - 1;
+    const int bound = d.R * (L + 1) + (d.n_pat > 0 ? max(0, L + 1 - d.n_pat) : 0);
+    if (w > d.k || best <= bound || best < kN - d.tmax) {
+      a.abort[c] = 1;  // exact (bound met or every message seen), or a witness
+    } else {
+      units = static_cast<unsigned long long>(d.H) * c_binom[d.k][w] * is_units_per_support(w);
+    }
+  }
+  a.is_units[c] = units;
+}
+
+// Task size of level w (units per task, sized so the level has about eight
+// tasks per resident thread) and the per-code task offsets.  One CTA.
+__global__ void __launch_bounds__(kScanThreads) scan_level_kernel(DistArgs a, int w) {
   __shared__ unsigned long long s_part[kScanThreads / 32];
+  __shared__ unsigned long long s_nb;
   __shared__ int s_over;
   const int t = threadIdx.x;
-  const long long N = static_cast<long long>(a.n) * a.k_max;
+  const int lane = t & 31, wid = t >> 5;
+  const int n = a.n;
   if (t == 0) s_over = 0;
   __syncthreads();
-  const long long chunk = (N + kScanThreads - 1) / kScanThreads;
-  const long long beg = min(N, t * chunk);
-  const long long end = min(N, beg + chunk);
+  const int chunk = (n + kScanThreads - 1) / kScanThreads;
+  const int beg = min(n, t * chunk);
+  const int end = min(n, beg + chunk);
+  // pass 1: total units
   unsigned long long sum = 0ull;
   bool over = false;
-  for (long long i = beg; i < end; ++i) {
-    const unsigned long long x = a.is_cnt[i];
+  for (int i = beg; i < end; ++i) {
+    const unsigned long long x = a.is_units[i];
     if (sum + x < sum) over = true;
     sum += x;
   }
-  const int lane = t & 31, wid = t >> 5;
-  unsigned long long incl = sum;
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long y = __shfl_xor_sync(0xffffffffu, sum, o);
+    if (sum + y < sum) over = true;
+    sum += y;
+  }
+  if (lane == 0) s_part[wid] = sum;
+  if (over) s_over = 1;
+  __syncthreads();
+  if (t == 0) {
+    unsigned long long tot = 0ull;
+    for (int i = 0; i < kScanThreads / 32; ++i) {
+      if (tot + s_part[i] < tot) s_over = 1;
+      tot += s_part[i];
+    }
+    const unsigned long long target = 8ull * static_cast<unsigned long long>(a.is_lanes);
+    unsigned long long nb = (tot + target - 1ull) / target;
+    s_nb = max(1ull, min(nb, is_max_task_units(w)));
+  }
+  __syncthreads();
+  const unsigned long long nb = s_nb;
+  // pass 2: tasks per code, exclusive scan
+  unsigned long long tsum = 0ull;
+  for (int i = beg; i < end; ++i) tsum += (a.is_units[i] + nb - 1ull) / nb;
+  unsigned long long incl = tsum;
   for (int o = 1; o < 32; o <<= 1) {
     const unsigned long long y = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) {
-      if (incl + y < incl) over = true;
-      incl += y;
-    }
+    if (lane >= o) incl += y;
   }
+  __syncthreads();
   if (lane == 31) s_part[wid] = incl;
-  if (over) s_over = 1;
   __syncthreads();
   if (wid == 0) {
     unsigned long long v = s_part[lane];
-    bool ov = false;
     for (int o = 1; o < 32; o <<= 1) {
       const unsigned long long y = __shfl_up_sync(0xffffffffu, v, o);
-      if (lane >= o) {
-        if (v + y < v) ov = true;
-        v += y;
-      }
+      if (lane >= o) v += y;
     }
-    if (ov) s_over = 1;
     s_part[lane] = v;
   }
   __syncthreads();
-  unsigned long long run = incl - sum + (wid > 0 ? s_part[wid - 1] : 0ull);
-  for (long long i = beg; i < end; ++i) {
+  unsigned long long run = incl - tsum + (wid > 0 ? s_part[wid - 1] : 0ull);
+  for (int i = beg; i < end; ++i) {
     a.is_off[i] = run;
-    run += a.is_cnt[i];
-  }
-  if (t == kScanThreads - 1) {
-    a.is_off[N] = s_part[31];
-    a.is_hdr->total_tasks = s_part[31];
-    a.is_hdr->counter = 0ull;
+    run += (a.is_units[i] + nb - 1ull) / nb;
   }
   __syncthreads();
-  if (t == 0 && s_over) {
-    // Work beyond 2^64 tasks: nothing runs.
-    for (long long i = 0; i <= N; ++i) a.is_off[i] = 0ull;
-    a.is_hdr->total_tasks = 0ull;
-    report_status(a.hdr, TG_ERR_INVALID_ARGUMENT);
+  if (t == 0) {
+    unsigned long long total = s_part[31];
+    if (s_over) {
+      // Work beyond 2^64 units: nothing runs.
+      for (int i = 0; i <= n; ++i) a.is_off[i] = 0ull;
+      total = 0ull;
+      report_status(a.hdr, TG_ERR_INVALID_ARGUMENT);
+    }
+    a.is_off[n] = total;
+    a.is_hdr->counter = 0ull;
+    a.is_hdr->total = total;
+    a.is_hdr->units = nb;
+    a.is_hdr->level = w;
+    a.is_hdr->tasks_all += total;
   }
 }
-
-// ---------------------------------------------------------------------------
-// Walk.
-// ---------------------------------------------------------------------------
 
 __device__ __forceinline__ void is_weight(const V6& p, int& wmin) {
   const int lo = __popc(lop3<0xFE>(p.l0, p.l1, p.l2));
@@ -358,33 +375,43 @@ __device__ __forceinline__ void is_weight(const V6& p, int& wmin) {
   wmin = __viaddmin_s32(lo, hi, wmin);
 }
 
-// p <- alpha p on the bit-sliced planes.
-__device__ __forceinline__ void v6_alpha(V6& p) {
-  uint32_t t = p.l2;
-  p.l2 = p.l1;
-  p.l1 = p.l0 ^ t;
-  p.l0 = t;
-  t = p.h2;
-  p.h2 = p.h1;
-  p.h1 = p.h0 ^ t;
-  p.h0 = t;
+// p <- alpha^e p on the bit-sliced planes, e in 0..6.
+__device__ __forceinline__ void v6_alpha_pow(V6& p, int e) {
+  for (int i = 0; i < e; ++i) {
+    uint32_t t = p.l2;
+    p.l2 = p.l1;
+    p.l1 = p.l0 ^ t;
+    p.l0 = t;
+    t = p.h2;
+    p.h2 = p.h1;
+    p.h1 = p.h0 ^ t;
+    p.h0 = t;
+  }
 }
 
-// Delta of the move between 49-codeword blocks b - 1 and b (b >= 1): digit
-// 2 + tz moves, tz = trailing base-7 zeros of b.  It runs up when the digits
-// above it sum to an even number, between alpha^v and alpha^(v+1).
-__device__ __forceinline__ const V6* is_block_move(const V6* rows, unsigned b, uint32_t r2,
-                                                  uint32_t r3, uint32_t r4) {
-  unsigned q = b;
+// Gray value of digit 2 + i at the start of block b: the base-7 digit o_i of
+// b, reflected (6 - o_i) when the digits above it sum to an odd number.
+__device__ __forceinline__ int is_block_digit(unsigned long long& rest) {
+  const int o = int(rest % 7ull);
+  rest /= 7ull;
+  return (rest & 1ull) ? 6 - o : o;
+}
+
+// Delta of the move from block b - 1 to block b (b >= 1): digit 2 + tz moves,
+// tz = trailing base-7 zeros of b, up when the digits above it sum to an even
+// number, between alpha^v and alpha^(v+1).  dig[i * kStride] is the row of
+// digit 2 + i.
+template <int kStride>
+__device__ __forceinline__ const V6* is_block_move(const V6* rows, const uint16_t* dig,
+                                                  unsigned long long b) {
   int tz = 0;
-  while (q % 7u == 0u) {
-    q /= 7u;
+  while (b % 7ull == 0ull) {
+    b /= 7ull;
     ++tz;
   }
-  const unsigned ot = q % 7u;
-  const int v = ((q / 7u) & 1u) ? int(6u - ot) : int(ot - 1u);
-  const uint32_t R = tz == 0 ? r2 : (tz == 1 ? r3 : r4);
-  return rows + R + 1 + v;
+  const int ot = int(b % 7ull);
+  const int v = ((b / 7ull) & 1ull) ? 6 - ot : ot - 1;
+  return rows + dig[tz * kStride] + 1 + v;
 }
 
 #define TG_IS_STEP(D) \
@@ -395,42 +422,35 @@ __device__ __forceinline__ const V6* is_block_move(const V6* rows, unsigned b, u
 #define TG_IS_SWEEP_DOWN \
   TG_IS_STEP(d5); TG_IS_STEP(d4); TG_IS_STEP(d3); TG_IS_STEP(d2); TG_IS_STEP(d1); TG_IS_STEP(d0)
 
-// Walks the 7^inner codewords of one support from cw (every walked
-// coefficient alpha^0).  Digit 0 (row r0) and digit 1 (row r1) keep their six
-// deltas in registers, so the walk is straight-line code over blocks of 49
-// codewords; the one move between blocks (digits 2..4, rows r2..r4) is loaded
-// a block ahead.  Rows are vector offsets from `rows`.  Returns the codewords
-// evaluated.
-__device__ __forceinline__ unsigned long long is_walk_support(V6 cw, int inner, const V6* rows,
-                                                              uint32_t r0, uint32_t r1,
-                                                              uint32_t r2, uint32_t r3,
-                                                              uint32_t r4, int wthr,
-                                                              const int32_t* stop, int& wmin) {
-  is_weight(cw, wmin);
-  if (inner == 0) return 1ull;
+// Walks blocks [b0, b0 + nblk) of one support from cw, the codeword at the
+// start of block b0.  Digits 0 (row r0) and 1 (row r1) keep their six deltas
+// in registers, so each block is 49 codewords of straight-line code; the move
+// between blocks (digits 2.., rows dig[]) is loaded a block ahead.  Returns
+// the codewords evaluated.
+template <int kStride>
+__device__ __forceinline__ unsigned long long is_walk_blocks(
+    V6 cw, const V6* rows, uint32_t r0, uint32_t r1, const uint16_t* dig, unsigned long long b0,
+    unsigned long long nblk, int wthr, const int32_t* stop, int& wmin) {
   const V6* R0 = rows + r0;
   const V6 d0 = v6_ldg(R0 + 1), d1 = v6_ldg(R0 + 2), d2 = v6_ldg(R0 + 3);
   const V6 d3 = v6_ldg(R0 + 4), d4 = v6_ldg(R0 + 5), d5 = v6_ldg(R0 + 6);
-  if (inner == 1) {
-    TG_IS_SWEEP_UP;
-    return 7ull;
-  }
   const V6* R1 = rows + r1;
   const V6 e0 = v6_ldg(R1 + 1), e1 = v6_ldg(R1 + 2), e2 = v6_ldg(R1 + 3);
   const V6 e3 = v6_ldg(R1 + 4), e4 = v6_ldg(R1 + 5), e5 = v6_ldg(R1 + 6);
-  const unsigned blocks = static_cast<unsigned>(c_pow7[inner - 2]);
+  is_weight(cw, wmin);
   V6 nx;
   v6_zero(nx);
-  if (blocks > 1u) nx = v6_ldg(is_block_move(rows, 1u, r2, r3, r4));
-  unsigned b = 0;
-  for (; b < blocks; ++b) {
-    if (b) {
+  if (nblk > 1ull) nx = v6_ldg(is_block_move<kStride>(rows, dig, b0 + 1ull));
+  unsigned long long i = 0;
+  for (; i < nblk; ++i) {
+    const unsigned long long b = b0 + i;
+    if (i) {
       TG_IS_STEP(nx);
-      if (b + 1u < blocks) nx = v6_ldg(is_block_move(rows, b + 1u, r2, r3, r4));
+      if (i + 1ull < nblk) nx = v6_ldg(is_block_move<kStride>(rows, dig, b + 1ull));
     }
     // Digit 0 runs up in sweep s of block b when b + s is even; digit 1 runs
     // up through the block when b is even.
-    if ((b & 1u) == 0u) {
+    if ((b & 1ull) == 0ull) {
       TG_IS_SWEEP_UP;   TG_IS_STEP(e0);
       TG_IS_SWEEP_DOWN; TG_IS_STEP(e1);
       TG_IS_SWEEP_UP;   TG_IS_STEP(e2);
@@ -448,136 +468,136 @@ __device__ __forceinline__ unsigned long long is_walk_support(V6 cw, int inner, 
       TG_IS_SWEEP_DOWN;
     }
     if (wmin < wthr) break;
-    if ((b & 15u) == 15u && ld_flag(stop)) break;
+    if ((i & 15ull) == 15ull && ld_flag(stop)) break;
   }
-  return 49ull * (min(b, blocks - 1u) + 1u);
+  return 49ull * (min(i, nblk - 1ull) + 1ull);
 }
 
 #undef TG_IS_SWEEP_DOWN
 #undef TG_IS_SWEEP_UP
 #undef TG_IS_STEP
 
-// One task: its supports walked completely; the smallest weight met, and the
-// codewords evaluated in ncw.
-__device__ __forceinline__ int is_task(const DistArgs& a,
-                                       const unsigned long long (*bn)[kIsBinom], int c, int k,
-                                       int w, unsigned long long local, int wthr,
-                                       unsigned long long& ncw) {
+// Units [u0, u1) of code c at level w (flat over set, support, block); the
+// smallest weight met, and the codewords evaluated in ncw.  dig (stride
+// kStride) is this thread's scratch for the rows of digits 2..w-2.
+template <int kStride>
+__device__ __forceinline__ int is_walk_units(const DistArgs& a,
+                                             const unsigned long long (*bn)[kIsBinom],
+                                             uint16_t* dig, int c, int k, int w,
+                                             unsigned long long u0, unsigned long long u1,
+                                             int wthr, unsigned long long& ncw) {
   const unsigned long long n_sup = bn[k][w];
-  const IsTaskShape sh = is_task_shape(n_sup, w);
-  const int j = int(local / sh.per_set);
-  const unsigned long long rr = local - static_cast<unsigned long long>(j) * sh.per_set;
-  const unsigned long long B = c_pow7[sh.outer];
-  // supports [s_beg, s_end) of C(k, w) <= C(21, 10) fit 32 bits
-  uint32_t s_beg, s_end;
-  unsigned long long blk0;
-  if (sh.outer > 0) {
-    s_beg = uint32_t(rr / B);
-    s_end = s_beg + 1u;
-    blk0 = rr - static_cast<unsigned long long>(s_beg) * B;
-  } else {
-    s_beg = uint32_t(rr * sh.group);
-    s_end = uint32_t(min(rr * sh.group + sh.group, n_sup));
-    blk0 = 0ull;
-  }
-  const V6* rows = a.is_rows + size_t(c) * a.is_stride + size_t(j) * k * kIsVecPerRow;
+  const unsigned long long bps = is_units_per_support(w);
+  const unsigned long long per_set = n_sup * bps;
+  const V6* base = a.is_rows + size_t(c) * a.is_stride;
   const int32_t* stop = a.abort + c;
   int wmin = 64;
   ncw = 0ull;
-  for (uint32_t s = s_beg; s < s_end; ++s) {
+  unsigned long long u = u0;
+  while (u < u1) {
+    const unsigned long long j = u / per_set;
+    const unsigned long long r = u - j * per_set;
+    const unsigned long long s = r / bps;
+    const unsigned long long b = r - s * bps;
+    const unsigned long long nblk = min(bps - b, u1 - u);
+    const V6* rows = base + size_t(j) * k * kIsVecPerRow;
     // Support rows from the largest down (combinadic unranking).  The q-th
-    // row found is inner digit q while q < inner, then the outer rows from the
-    // top block digit down, and last the row with coefficient 1.
+    // row found is Gray digit q (q < w - 1); the last one has coefficient 1.
+    // Digits 0 and 1 start at alpha^0 (b even) or alpha^6 (b odd); digit
+    // 2 + i starts at the Gray value of base-7 digit i of b.
     V6 cw;
     v6_zero(cw);
-    uint32_t r0 = 0u, r1 = 0u, r2 = 0u, r3 = 0u, r4 = 0u;
-    unsigned long long srank = s, blk = blk0;
-    unsigned long long P = sh.outer > 0 ? c_pow7[sh.outer - 1] : 1ull;
+    uint32_t r0 = 0u, r1 = 0u;
+    unsigned long long srank = s, rest = b;
+    const int e01 = (b & 1ull) ? 6 : 0;
     int rem = w, q = 0;
     for (int pos = k - 1; pos >= 0 && rem > 0; --pos) {
-      const unsigned long long b = bn[pos][rem];
-      if (srank < b) continue;
-      srank -= b;
+      const unsigned long long bb = bn[pos][rem];
+      if (srank < bb) continue;
+      srank -= bb;
       --rem;
       const uint32_t R = uint32_t(pos * kIsVecPerRow);
       V6 g = v6_ldg(rows + R);
-      if (q < sh.inner) {
-        if (q == 0) r0 = R;
-        else if (q == 1) r1 = R;
-        else if (q == 2) r2 = R;
-        else if (q == 3) r3 = R;
-        else r4 = R;
-      } else if (rem > 0) {
-        const unsigned long long e = blk / P;
-        blk -= e * P;
-        P /= 7ull;
-        for (unsigned long long i = 0; i < e; ++i) v6_alpha(g);
+      if (rem > 0) {
+        int e;
+        if (q == 0) {
+          r0 = R;
+          e = w >= 3 ? e01 : 0;
+        } else if (q == 1) {
+          r1 = R;
+          e = e01;
+        } else {
+          dig[(q - 2) * kStride] = uint16_t(R);
+          e = is_block_digit(rest);
+        }
+        v6_alpha_pow(g, e);
       }
       v6_xor(cw, g);
       ++q;
     }
-    ncw += is_walk_support(cw, sh.inner, rows, r0, r1, r2, r3, r4, wthr, stop, wmin);
+    if (w == 1) {
+      is_weight(cw, wmin);
+      ncw += 1ull;
+    } else if (w == 2) {
+      const V6* R0 = rows + r0;
+      is_weight(cw, wmin);
+      for (int v = 0; v < 6; ++v) {
+        v6_xor(cw, v6_ldg(R0 + 1 + v));
+        is_weight(cw, wmin);
+      }
+      ncw += 7ull;
+    } else {
+      ncw += is_walk_blocks<kStride>(cw, rows, r0, r1, dig, b, nblk, wthr, stop, wmin);
+    }
+    u += nblk;
     if (wmin < wthr) break;
   }
   return wmin;
 }
 
-// Marks code c finished and moves the counter past its current level range.
-__device__ __forceinline__ void is_finish(const DistArgs& a, int c, unsigned long long range_end) {
-  atomicExch(a.abort + c, 1);
-  atomicMax(&a.is_hdr->counter, range_end);
-}
+constexpr int kIsMaxDigits = kMaxExactK - 3;  // digits 2..w-2, w <= 21
 
 template <int kTPB, int kMinBlocks>
-__global__ void __launch_bounds__(kTPB, kMinBlocks) walk_infoset_kernel(DistArgs a) {
+__global__ void __launch_bounds__(kTPB, kMinBlocks) walk_level_kernel(DistArgs a, int w) {
   __shared__ unsigned long long s_binom[kIsBinom][kIsBinom];
+  __shared__ uint16_t s_dig[kIsMaxDigits][kTPB];
   for (int i = threadIdx.x; i < kIsBinom * kIsBinom; i += kTPB)
     s_binom[i / kIsBinom][i % kIsBinom] = c_binom[i / kIsBinom][i % kIsBinom];
   __syncthreads();
   const int lane = threadIdx.x & 31;
-  const unsigned long long total = a.is_hdr->total_tasks;
-  const int NW = a.n * a.k_max;
+  const unsigned long long total = a.is_hdr->total;
+  const unsigned long long nb = a.is_hdr->units;
   unsigned long long evaluated = 0ull;
+  uint16_t* my_dig = &s_dig[0][threadIdx.x];  // this thread's digit rows, stride kTPB
   for (;;) {
     unsigned long long base = 0ull;
     if (lane == 0) base = atomicAdd(&a.is_hdr->counter, 32ull);
     base = __shfl_sync(0xffffffffu, base, 0);
     if (base >= total) break;
-    int f0 = 0;
-    if (lane == 0) f0 = last_le(a.is_off, NW + 1, base);
-    f0 = __shfl_sync(0xffffffffu, f0, 0);
+    int c0 = 0;
+    if (lane == 0) c0 = last_le(a.is_off, a.n + 1, base);
+    c0 = __shfl_sync(0xffffffffu, c0, 0);
     const unsigned long long t = base + lane;
     if (t >= total) continue;
-    const int f = t < __ldg(a.is_off + f0 + 1) ? f0 : last_le(a.is_off, NW + 1, t);
-    const int w = f / a.n + 1;
-    const int c = f - (w - 1) * a.n;
-    const unsigned long long r_beg = __ldg(a.is_off + f), r_end = __ldg(a.is_off + f + 1);
+    const int c = t < __ldg(a.is_off + c0 + 1) ? c0 : last_le(a.is_off, a.n + 1, t);
+    const unsigned long long r_end = __ldg(a.is_off + c + 1);
     if (ld_flag(a.abort + c)) {
       atomicMax(&a.is_hdr->counter, r_end);
       continue;
     }
     const int wthr = kN - a.desc[c].tmax;
+    const unsigned long long u0 = (t - __ldg(a.is_off + c)) * nb;
+    const unsigned long long u1 = min(u0 + nb, static_cast<unsigned long long>(a.is_units[c]));
     unsigned long long ncw = 0ull;
-    const int wmin = is_task(a, s_binom, c, a.desc[c].k, w, t - r_beg, wthr, ncw);
+    const int wmin = is_walk_units<kTPB>(a, s_binom, my_dig, c, a.desc[c].k, w, u0, u1, wthr, ncw);
     evaluated += ncw;
     const int best = min(atomicMin(a.is_best + c, wmin), wmin);
     if (best < wthr) {
-      is_finish(a, c, r_end);  // a witness below the target distance
-      continue;
-    }
-    __threadfence();
-    if (atomicAdd(a.is_done + f, 1ull) + 1ull == __ldg(a.is_cnt + f)) {
-      // The last task of level w: check the bound of the complete levels.
-      const unsigned bit = 1u << (w - 1);
-      const unsigned bits = atomicOr(a.is_bits + c, bit) | bit;
-      const int L = __ffs(~bits) - 1;
-      const int now = atomicAdd(a.is_best + c, 0);
-      const CodeDesc d = a.desc[c];
-      const int bound = d.R * (L + 1) + (d.n_pat > 0 ? max(0, L + 1 - d.n_pat) : 0);
-      if (L >= d.k || now <= bound) is_finish(a, c, r_end);
+      // a witness below the target distance: the code is decided
+      atomicExch(a.abort + c, 1);
+      atomicMax(&a.is_hdr->counter, r_end);
     }
   }
-  // codewords evaluated, one atomic per warp
   for (int o = 16; o > 0; o >>= 1) evaluated += __shfl_xor_sync(0xffffffffu, evaluated, o);
   if (lane == 0 && evaluated) atomicAdd(&a.is_hdr->codewords, evaluated);
 }
