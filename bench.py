@@ -40,7 +40,9 @@ METRIC = "GF(8) codewords/s, reference-equivalent (8^k-1 messages per code), bat
 UNIT = "codewords/s"
 WORKLOAD = "batched uneven evaluation: 10,000 seeded random P, |P|~U{6..14}, td=1, exact"
 POPC_PER_CODEWORD = 14.0 / 8.0  # histogram walk: 7 bins x 2 words per 8 codewords
-POPC_PER_CODEWORD_INFOSET = 2.0  # information-set walk: one weight per codeword
+# information-set walk: per sweep of 7 codewords, 7 selection counts on the
+# low 32 columns plus one count of the zero columns of the swept row
+POPC_PER_CODEWORD_INFOSET = 8.0 / 7.0
 
 
 def launches_per_step(k_max: int) -> int:
@@ -575,7 +577,8 @@ def run_b200_arm(args, d: Dist) -> None:
         dominant = {"kernel": "walk_infoset_kernel (+ finalize_infoset_kernel)",
                     "seconds": is_s, "codewords": paths["infoset_codewords"],
                     "popc_per_codeword": POPC_PER_CODEWORD_INFOSET,
-                    "note": "2 POPC per codeword (one per 32-bit half of the nonzero mask)"}
+                    "note": "8 POPC per 7 codewords (seven zero-selection counts on the low "
+                            "32 columns in the W = P / g domain, one count of g's zero columns)"}
     else:
         dominant = {"kernel": "walk_hist_kernel", "seconds": enum_s,
                     "codewords": paths["enumeration_codewords"],

@@ -143,6 +143,31 @@ __device__ int is_gauss_jordan(int lane, int k, uint64_t& p0, uint64_t& p1, uint
   return rank;
 }
 
+// Reorders the 49 columns of a bit-sliced row: the columns outside `piv`
+// first (increasing), then those in `piv`.  Weights do not depend on the
+// column order, and a set's codewords are sparse on its own pivot columns;
+// with those last, the low 32 columns look like random columns, so the walk's
+// low-half weight bound is tight.
+__device__ __forceinline__ void is_reorder_columns(uint64_t piv, uint64_t& p0, uint64_t& p1,
+                                                   uint64_t& p2) {
+  uint64_t q0 = 0ull, q1 = 0ull, q2 = 0ull;
+  uint64_t rest = ~piv & kMask49;
+  uint64_t tail = piv & kMask49;
+  for (int d = 0; d < kN; ++d) {
+    const bool front = rest != 0ull;
+    const uint64_t pick = front ? rest : tail;
+    const int col = __ffsll(static_cast<long long>(pick)) - 1;
+    if (front) rest &= rest - 1ull;
+    else tail &= tail - 1ull;
+    q0 |= ((p0 >> col) & 1ull) << d;
+    q1 |= ((p1 >> col) & 1ull) << d;
+    q2 |= ((p2 >> col) & 1ull) << d;
+  }
+  p0 = q0;
+  p1 = q1;
+  p2 = q2;
+}
+
 // Writes the rows of one set: g and the six Gray-step deltas per row.
 __device__ __forceinline__ void is_store_set(V6* dst, int lane, int k, uint64_t p0, uint64_t p1,
                                              uint64_t p2) {
@@ -219,9 +244,12 @@ __global__ void __launch_bounds__(kIsPrepWarps * 32) prep_infoset_kernel(DistArg
     uint64_t p0 = o0, p1 = o1, p2 = o2, used = 0ull;
     V6* base = a.is_rows + size_t(c) * a.is_stride;
     while (n_sets < cap_sets) {
+      const uint64_t used_before = used;
       const int r = is_gauss_jordan(lane, k, p0, p1, p2, used, s_ord[wl]);
       if (r < k && (r == 0 || k - r > kIsMaxDelta)) break;
-      is_store_set(base + size_t(n_sets) * k * kIsVecPerRow, lane, k, p0, p1, p2);
+      uint64_t q0 = p0, q1 = p1, q2 = p2;
+      is_reorder_columns(used & ~used_before, q0, q1, q2);
+      is_store_set(base + size_t(n_sets) * k * kIsVecPerRow, lane, k, q0, q1, q2);
       ++n_sets;
       if (r < k) {
         delta = k - r;
@@ -414,30 +442,123 @@ __device__ __forceinline__ const V6* is_block_move(const V6* rows, const uint16_
   return rows + dig[tz * kStride] + 1 + v;
 }
 
-#define TG_IS_STEP(D) \
-  v6_xor(cw, D);      \
-  is_weight(cw, wmin)
-#define TG_IS_SWEEP_UP \
-  TG_IS_STEP(d0); TG_IS_STEP(d1); TG_IS_STEP(d2); TG_IS_STEP(d3); TG_IS_STEP(d4); TG_IS_STEP(d5)
-#define TG_IS_SWEEP_DOWN \
-  TG_IS_STEP(d5); TG_IS_STEP(d4); TG_IS_STEP(d3); TG_IS_STEP(d2); TG_IS_STEP(d1); TG_IS_STEP(d0)
+// Exact weights of the seven codewords P + alpha^v g, v = 0..6, min'd into
+// wmin.
+__device__ __noinline__ int is_sweep_exact(V6 P, const V6* g_row, int wmin) {
+  V6 g = v6_ldg(g_row);
+  for (int v = 0; v < 7; ++v) {
+    const int lo = __popc(lop3<0xFE>(P.l0 ^ g.l0, P.l1 ^ g.l1, P.l2 ^ g.l2));
+    const int hi = __popc(lop3<0xFE>(P.h0 ^ g.h0, P.h1 ^ g.h1, P.h2 ^ g.h2));
+    wmin = min(wmin, lo + hi);
+    v6_alpha_pow(g, 1);
+  }
+  return wmin;
+}
 
-// Walks blocks [b0, b0 + nblk) of one support from cw, the codeword at the
-// start of block b0.  Digits 0 (row r0) and 1 (row r1) keep their six deltas
-// in registers, so each block is 49 codewords of straight-line code; the move
-// between blocks (digits 2.., rows dig[]) is loaded a block ahead.  Returns
-// the codewords evaluated.
+// Three bit planes of 32 columns of GF(8) values.
+struct Pl3 {
+  uint32_t x0, x1, x2;
+};
+
+// Column-wise product modulo x^3 + x + 1.
+__device__ __forceinline__ Pl3 pl3_mul(const Pl3& a, const Pl3& b) {
+  const uint32_t t0 = a.x0 & b.x0;
+  const uint32_t t1 = lop3<0x6A>(a.x0, b.x1, a.x1 & b.x0);  // (a & b) ^ c
+  const uint32_t t2 = lop3<0x6A>(a.x0, b.x2, lop3<0x6A>(a.x1, b.x1, a.x2 & b.x0));
+  const uint32_t t3 = lop3<0x6A>(a.x1, b.x2, a.x2 & b.x1);
+  const uint32_t t4 = a.x2 & b.x2;
+  return Pl3{t0 ^ t3, lop3<0x96>(t1, t3, t4), t2 ^ t4};
+}
+
+// Column-wise inverse x^6 = x^2 x^4 (0 stays 0); squaring is linear.
+__device__ __forceinline__ Pl3 pl3_inv(const Pl3& a) {
+  const Pl3 s2{a.x0, a.x2, a.x1 ^ a.x2};
+  const Pl3 s4{s2.x0, s2.x2, s2.x1 ^ s2.x2};
+  return pl3_mul(s2, s4);
+}
+
+__device__ __forceinline__ Pl3 pl3_lo(const V6& v) { return Pl3{v.l0, v.l1, v.l2}; }
+
+__device__ __forceinline__ Pl3 pl3_and(const Pl3& a, uint32_t m) {
+  return Pl3{a.x0 & m, a.x1 & m, a.x2 & m};
+}
+
+__device__ __forceinline__ void pl3_xor(Pl3& a, const Pl3& b) {
+  a.x0 ^= b.x0;
+  a.x1 ^= b.x1;
+  a.x2 ^= b.x2;
+}
+
+// The rare path of a sweep: rebuilds P (the support's rows other than digit
+// 0 at digit-1 value v1 and the block-b values of digits 2..) and counts the
+// seven codewords exactly.
+template <int kStride>
+__device__ __noinline__ int is_sweep_rebuild(const V6* rows, uint32_t r0, uint32_t r1,
+                                             uint32_t rc, const uint16_t* dig, int n_dig,
+                                             unsigned long long b, int v1, int wmin) {
+  V6 P = v6_ldg(rows + rc);
+  V6 x = v6_ldg(rows + r1);
+  v6_alpha_pow(x, v1);
+  v6_xor(P, x);
+  unsigned long long rest = b;
+  for (int i = 0; i < n_dig; ++i) {
+    V6 y = v6_ldg(rows + dig[i * kStride]);
+    v6_alpha_pow(y, is_block_digit(rest));
+    v6_xor(P, y);
+  }
+  return is_sweep_exact(P, rows + r0, wmin);
+}
+
+// One sweep of digit 0 at digit-1 value V1, on the low 32 columns in the
+// domain W = P / g (column-wise; g the digit-0 row): P + alpha^v g vanishes
+// at column j exactly when W_j = alpha^v (g_j != 0) or P_j = 0 (g_j = 0).  So
+// the zeros of all seven codewords are seven one-LOP3 selections plus the
+// zero columns of g (tracked as Pz = P & gz).  The high columns hold the
+// set's pivot columns, where a codeword equals its message, so they weigh at
+// least hb; a sweep whose lightest low half plus hb is below wmin is counted
+// exactly on the rare path.
+#define TG_IS_SWEEP(V1)                                                                        \
+  {                                                                                            \
+    const int z0_ = __popc(lop3<sel_lut(1)>(W.x0, W.x1, W.x2));                                \
+    const int z1_ = __popc(lop3<sel_lut(2)>(W.x0, W.x1, W.x2));                                \
+    const int z2_ = __popc(lop3<sel_lut(4)>(W.x0, W.x1, W.x2));                                \
+    const int z3_ = __popc(lop3<sel_lut(3)>(W.x0, W.x1, W.x2));                                \
+    const int z4_ = __popc(lop3<sel_lut(6)>(W.x0, W.x1, W.x2));                                \
+    const int z5_ = __popc(lop3<sel_lut(7)>(W.x0, W.x1, W.x2));                                \
+    const int z6_ = __popc(lop3<sel_lut(5)>(W.x0, W.x1, W.x2));                                \
+    const int zm_ = __vimax3_s32(__vimax3_s32(z0_, z1_, z2_), __vimax3_s32(z3_, z4_, z5_), z6_); \
+    const int zz_ = ngz - __popc(lop3<0xFE>(Pz.x0, Pz.x1, Pz.x2));                            \
+    if (32 - zm_ - zz_ + hb < wmin)                                                            \
+      wmin = is_sweep_rebuild<kStride>(rows, r0, r1, rc, dig, n_dig, b, V1, wmin);              \
+  }
+#define TG_IS_MOVE(I) \
+  pl3_xor(W, E[I]);   \
+  pl3_xor(Pz, Z[I])
+
+// Walks blocks [b0, b0 + nblk) of one support; P is the sum of its rows other
+// than digit 0 at the start of block b0.  Each block is 7 sweeps of digit 0
+// (row r0) with digit 1 (row r1) moving between them: 49 codewords of
+// straight-line code with digit 1's six moves in registers.  The move between
+// blocks (digits 2.., rows dig[]) is loaded a block ahead.  Returns the
+// codewords evaluated.
 template <int kStride>
 __device__ __forceinline__ unsigned long long is_walk_blocks(
-    V6 cw, const V6* rows, uint32_t r0, uint32_t r1, const uint16_t* dig, unsigned long long b0,
-    unsigned long long nblk, int wthr, const int32_t* stop, int& wmin) {
-  const V6* R0 = rows + r0;
-  const V6 d0 = v6_ldg(R0 + 1), d1 = v6_ldg(R0 + 2), d2 = v6_ldg(R0 + 3);
-  const V6 d3 = v6_ldg(R0 + 4), d4 = v6_ldg(R0 + 5), d5 = v6_ldg(R0 + 6);
-  const V6* R1 = rows + r1;
-  const V6 e0 = v6_ldg(R1 + 1), e1 = v6_ldg(R1 + 2), e2 = v6_ldg(R1 + 3);
-  const V6 e3 = v6_ldg(R1 + 4), e4 = v6_ldg(R1 + 5), e5 = v6_ldg(R1 + 6);
-  is_weight(cw, wmin);
+    const V6& P, const V6* rows, uint32_t r0, uint32_t r1, uint32_t rc, const uint16_t* dig,
+    int n_dig, unsigned long long b0, unsigned long long nblk, int hb, int wthr,
+    const int32_t* stop, int& wmin) {
+  const Pl3 g = pl3_lo(v6_ldg(rows + r0));
+  const Pl3 h = pl3_inv(g);
+  const uint32_t gz = ~(g.x0 | g.x1 | g.x2);  // low columns where g is 0
+  const int ngz = __popc(gz);
+  Pl3 E[6], Z[6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+    const Pl3 d = pl3_lo(v6_ldg(rows + r1 + 1 + i));
+    E[i] = pl3_mul(d, h);
+    Z[i] = pl3_and(d, gz);
+  }
+  Pl3 W = pl3_mul(pl3_lo(P), h);
+  Pl3 Pz = pl3_and(pl3_lo(P), gz);
   V6 nx;
   v6_zero(nx);
   if (nblk > 1ull) nx = v6_ldg(is_block_move<kStride>(rows, dig, b0 + 1ull));
@@ -445,27 +566,20 @@ __device__ __forceinline__ unsigned long long is_walk_blocks(
   for (; i < nblk; ++i) {
     const unsigned long long b = b0 + i;
     if (i) {
-      TG_IS_STEP(nx);
+      const Pl3 d = pl3_lo(nx);
+      pl3_xor(W, pl3_mul(d, h));
+      pl3_xor(Pz, pl3_and(d, gz));
       if (i + 1ull < nblk) nx = v6_ldg(is_block_move<kStride>(rows, dig, b + 1ull));
     }
-    // Digit 0 runs up in sweep s of block b when b + s is even; digit 1 runs
-    // up through the block when b is even.
+    // digit 1 runs up through block b when b is even
     if ((b & 1ull) == 0ull) {
-      TG_IS_SWEEP_UP;   TG_IS_STEP(e0);
-      TG_IS_SWEEP_DOWN; TG_IS_STEP(e1);
-      TG_IS_SWEEP_UP;   TG_IS_STEP(e2);
-      TG_IS_SWEEP_DOWN; TG_IS_STEP(e3);
-      TG_IS_SWEEP_UP;   TG_IS_STEP(e4);
-      TG_IS_SWEEP_DOWN; TG_IS_STEP(e5);
-      TG_IS_SWEEP_UP;
+      TG_IS_SWEEP(0); TG_IS_MOVE(0); TG_IS_SWEEP(1); TG_IS_MOVE(1); TG_IS_SWEEP(2);
+      TG_IS_MOVE(2); TG_IS_SWEEP(3); TG_IS_MOVE(3); TG_IS_SWEEP(4); TG_IS_MOVE(4);
+      TG_IS_SWEEP(5); TG_IS_MOVE(5); TG_IS_SWEEP(6);
     } else {
-      TG_IS_SWEEP_DOWN; TG_IS_STEP(e5);
-      TG_IS_SWEEP_UP;   TG_IS_STEP(e4);
-      TG_IS_SWEEP_DOWN; TG_IS_STEP(e3);
-      TG_IS_SWEEP_UP;   TG_IS_STEP(e2);
-      TG_IS_SWEEP_DOWN; TG_IS_STEP(e1);
-      TG_IS_SWEEP_UP;   TG_IS_STEP(e0);
-      TG_IS_SWEEP_DOWN;
+      TG_IS_SWEEP(6); TG_IS_MOVE(5); TG_IS_SWEEP(5); TG_IS_MOVE(4); TG_IS_SWEEP(4);
+      TG_IS_MOVE(3); TG_IS_SWEEP(3); TG_IS_MOVE(2); TG_IS_SWEEP(2); TG_IS_MOVE(1);
+      TG_IS_SWEEP(1); TG_IS_MOVE(0); TG_IS_SWEEP(0);
     }
     if (wmin < wthr) break;
     if ((i & 15ull) == 15ull && ld_flag(stop)) break;
@@ -473,25 +587,26 @@ __device__ __forceinline__ unsigned long long is_walk_blocks(
   return 49ull * (min(i, nblk - 1ull) + 1ull);
 }
 
-#undef TG_IS_SWEEP_DOWN
-#undef TG_IS_SWEEP_UP
-#undef TG_IS_STEP
+#undef TG_IS_MOVE
+#undef TG_IS_SWEEP
 
 // Units [u0, u1) of code c at level w (flat over set, support, block); the
-// smallest weight met, and the codewords evaluated in ncw.  dig (stride
-// kStride) is this thread's scratch for the rows of digits 2..w-2.
+// smallest weight met (or wmin when none is smaller), and the codewords
+// evaluated in ncw.  dig (stride kStride) is this thread's scratch for the
+// rows of digits 2..w-2.
 template <int kStride>
 __device__ __forceinline__ int is_walk_units(const DistArgs& a,
                                              const unsigned long long (*bn)[kIsBinom],
                                              uint16_t* dig, int c, int k, int w,
                                              unsigned long long u0, unsigned long long u1,
-                                             int wthr, unsigned long long& ncw) {
+                                             int wthr, int wmin, unsigned long long& ncw) {
   const unsigned long long n_sup = bn[k][w];
   const unsigned long long bps = is_units_per_support(w);
   const unsigned long long per_set = n_sup * bps;
   const V6* base = a.is_rows + size_t(c) * a.is_stride;
   const int32_t* stop = a.abort + c;
-  int wmin = 64;
+  const int n_sets = a.desc[c].H;
+  const int delta = a.desc[c].n_pat;  // rank deficit of the last set (0: full)
   ncw = 0ull;
   unsigned long long u = u0;
   while (u < u1) {
@@ -502,14 +617,14 @@ __device__ __forceinline__ int is_walk_units(const DistArgs& a,
     const unsigned long long nblk = min(bps - b, u1 - u);
     const V6* rows = base + size_t(j) * k * kIsVecPerRow;
     // Support rows from the largest down (combinadic unranking).  The q-th
-    // row found is Gray digit q (q < w - 1); the last one has coefficient 1.
-    // Digits 0 and 1 start at alpha^0 (b even) or alpha^6 (b odd); digit
+    // row found is Gray digit q (q < w - 1); the last one (rc) has
+    // coefficient 1.  Digit 0 is swept through all seven values and stays out
+    // of P; digit 1 starts at alpha^0 (b even) or alpha^6 (b odd); digit
     // 2 + i starts at the Gray value of base-7 digit i of b.
-    V6 cw;
-    v6_zero(cw);
-    uint32_t r0 = 0u, r1 = 0u;
+    V6 P;
+    v6_zero(P);
+    uint32_t r0 = 0u, r1 = 0u, rc = 0u;
     unsigned long long srank = s, rest = b;
-    const int e01 = (b & 1ull) ? 6 : 0;
     int rem = w, q = 0;
     for (int pos = k - 1; pos >= 0 && rem > 0; --pos) {
       const unsigned long long bb = bn[pos][rem];
@@ -517,37 +632,42 @@ __device__ __forceinline__ int is_walk_units(const DistArgs& a,
       srank -= bb;
       --rem;
       const uint32_t R = uint32_t(pos * kIsVecPerRow);
-      V6 g = v6_ldg(rows + R);
-      if (rem > 0) {
-        int e;
-        if (q == 0) {
-          r0 = R;
-          e = w >= 3 ? e01 : 0;
-        } else if (q == 1) {
-          r1 = R;
-          e = e01;
+      if (rem > 0 && q == 0) {
+        r0 = R;
+      } else {
+        V6 g = v6_ldg(rows + R);
+        if (rem > 0) {
+          int e;
+          if (q == 1) {
+            r1 = R;
+            e = (b & 1ull) ? 6 : 0;
+          } else {
+            dig[(q - 2) * kStride] = uint16_t(R);
+            e = is_block_digit(rest);
+          }
+          v6_alpha_pow(g, e);
         } else {
-          dig[(q - 2) * kStride] = uint16_t(R);
-          e = is_block_digit(rest);
+          rc = R;
         }
-        v6_alpha_pow(g, e);
+        v6_xor(P, g);
       }
-      v6_xor(cw, g);
       ++q;
     }
     if (w == 1) {
-      is_weight(cw, wmin);
+      const int wt = __popc(lop3<0xFE>(P.l0, P.l1, P.l2)) + __popc(lop3<0xFE>(P.h0, P.h1, P.h2));
+      wmin = min(wmin, wt);
       ncw += 1ull;
     } else if (w == 2) {
-      const V6* R0 = rows + r0;
-      is_weight(cw, wmin);
-      for (int v = 0; v < 6; ++v) {
-        v6_xor(cw, v6_ldg(R0 + 1 + v));
-        is_weight(cw, wmin);
-      }
+      wmin = is_sweep_exact(P, rows + r0, wmin);
       ncw += 7ull;
     } else {
-      ncw += is_walk_blocks<kStride>(cw, rows, r0, r1, dig, b, nblk, wthr, stop, wmin);
+      // Weight on the set's pivot columns: the message restricted to the rows
+      // with pivots (w, less the deficit of a partial set), less the pivots
+      // that do not fit in the 17 high columns (k > 17).
+      const int dj = int(j) == n_sets - 1 ? delta : 0;
+      const int hb = max(0, w - dj - max(0, (k - dj) - 17));
+      ncw += is_walk_blocks<kStride>(P, rows, r0, r1, rc, dig, w - 3, b, nblk, hb, wthr, stop,
+                                     wmin);
     }
     u += nblk;
     if (wmin < wthr) break;
@@ -589,7 +709,10 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) walk_level_kernel(DistArgs a
     const unsigned long long u0 = (t - __ldg(a.is_off + c)) * nb;
     const unsigned long long u1 = min(u0 + nb, static_cast<unsigned long long>(a.is_units[c]));
     unsigned long long ncw = 0ull;
-    const int wmin = is_walk_units<kTPB>(a, s_binom, my_dig, c, a.desc[c].k, w, u0, u1, wthr, ncw);
+    // Codewords no lighter than the code's best so far cannot change it, so
+    // the walk starts from that best.
+    const int wmin = is_walk_units<kTPB>(a, s_binom, my_dig, c, a.desc[c].k, w, u0, u1, wthr,
+                                         ld_flag(a.is_best + c), ncw);
     evaluated += ncw;
     const int best = min(atomicMin(a.is_best + c, wmin), wmin);
     if (best < wthr) {
