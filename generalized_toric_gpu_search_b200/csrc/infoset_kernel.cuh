@@ -489,47 +489,48 @@ __device__ __forceinline__ void pl3_xor(Pl3& a, const Pl3& b) {
   a.x2 ^= b.x2;
 }
 
-// The rare path of a sweep: rebuilds P (the support's rows other than digit
-// 0 at digit-1 value v1 and the block-b values of digits 2..) and counts the
-// seven codewords exactly.
+// The rare path of a block: rebuilds P (the support's rows other than digit
+// 0, at each digit-1 value and the block-b values of digits 2..) and counts
+// the block's 49 codewords exactly.
 template <int kStride>
-__device__ __noinline__ int is_sweep_rebuild(const V6* rows, uint32_t r0, uint32_t r1,
-                                             uint32_t rc, const uint16_t* dig, int n_dig,
-                                             unsigned long long b, int v1, int wmin) {
+__device__ __noinline__ int is_block_exact(const V6* rows, uint32_t r0, uint32_t r1, uint32_t rc,
+                                           const uint16_t* dig, int n_dig, unsigned long long b,
+                                           int wmin) {
   V6 P = v6_ldg(rows + rc);
-  V6 x = v6_ldg(rows + r1);
-  v6_alpha_pow(x, v1);
-  v6_xor(P, x);
   unsigned long long rest = b;
   for (int i = 0; i < n_dig; ++i) {
     V6 y = v6_ldg(rows + dig[i * kStride]);
     v6_alpha_pow(y, is_block_digit(rest));
     v6_xor(P, y);
   }
-  return is_sweep_exact(P, rows + r0, wmin);
+  V6 x = v6_ldg(rows + r1);  // digit 1 through alpha^0..alpha^6
+  for (int v1 = 0; v1 < 7; ++v1) {
+    V6 Q = P;
+    v6_xor(Q, x);
+    wmin = is_sweep_exact(Q, rows + r0, wmin);
+    v6_alpha_pow(x, 1);
+  }
+  return wmin;
 }
 
-// One sweep of digit 0 at digit-1 value V1, on the low 32 columns in the
-// domain W = P / g (column-wise; g the digit-0 row): P + alpha^v g vanishes
-// at column j exactly when W_j = alpha^v (g_j != 0) or P_j = 0 (g_j = 0).  So
-// the zeros of all seven codewords are seven one-LOP3 selections plus the
-// zero columns of g (tracked as Pz = P & gz).  The high columns hold the
-// set's pivot columns, where a codeword equals its message, so they weigh at
-// least hb; a sweep whose lightest low half plus hb is below wmin is counted
-// exactly on the rare path.
-#define TG_IS_SWEEP(V1)                                                                        \
-  {                                                                                            \
-    const int z0_ = __popc(lop3<sel_lut(1)>(W.x0, W.x1, W.x2));                                \
-    const int z1_ = __popc(lop3<sel_lut(2)>(W.x0, W.x1, W.x2));                                \
-    const int z2_ = __popc(lop3<sel_lut(4)>(W.x0, W.x1, W.x2));                                \
-    const int z3_ = __popc(lop3<sel_lut(3)>(W.x0, W.x1, W.x2));                                \
-    const int z4_ = __popc(lop3<sel_lut(6)>(W.x0, W.x1, W.x2));                                \
-    const int z5_ = __popc(lop3<sel_lut(7)>(W.x0, W.x1, W.x2));                                \
-    const int z6_ = __popc(lop3<sel_lut(5)>(W.x0, W.x1, W.x2));                                \
-    const int zm_ = __vimax3_s32(__vimax3_s32(z0_, z1_, z2_), __vimax3_s32(z3_, z4_, z5_), z6_); \
-    const int zz_ = ngz - __popc(lop3<0xFE>(Pz.x0, Pz.x1, Pz.x2));                            \
-    if (32 - zm_ - zz_ + hb < wmin)                                                            \
-      wmin = is_sweep_rebuild<kStride>(rows, r0, r1, rc, dig, n_dig, b, V1, wmin);              \
+// One sweep of digit 0, on the low 32 columns in the domain W = P / g
+// (column-wise; g the digit-0 row): P + alpha^v g vanishes at column j
+// exactly when W_j = alpha^v (g_j != 0) or P_j = 0 (g_j = 0).  So the zeros
+// of all seven codewords are seven one-LOP3 selections plus the zero columns
+// of g (tracked as Pz = P & gz).  bm keeps the most low-half zeros of the
+// block.
+#define TG_IS_SWEEP                                                                              \
+  {                                                                                              \
+    const int z0_ = __popc(lop3<sel_lut(1)>(W.x0, W.x1, W.x2));                                  \
+    const int z1_ = __popc(lop3<sel_lut(2)>(W.x0, W.x1, W.x2));                                  \
+    const int z2_ = __popc(lop3<sel_lut(4)>(W.x0, W.x1, W.x2));                                  \
+    const int z3_ = __popc(lop3<sel_lut(3)>(W.x0, W.x1, W.x2));                                  \
+    const int z4_ = __popc(lop3<sel_lut(6)>(W.x0, W.x1, W.x2));                                  \
+    const int z5_ = __popc(lop3<sel_lut(7)>(W.x0, W.x1, W.x2));                                  \
+    const int z6_ = __popc(lop3<sel_lut(5)>(W.x0, W.x1, W.x2));                                  \
+    const int zz_ = ngz - __popc(lop3<0xFE>(Pz.x0, Pz.x1, Pz.x2));                              \
+    bm = __vimax3_s32(bm, __vimax3_s32(z0_, z1_, z2_) + zz_,                                     \
+                      __vimax3_s32(z3_, z4_, max(z5_, z6_)) + zz_);                      \
   }
 #define TG_IS_MOVE(I) \
   pl3_xor(W, E[I]);   \
@@ -572,15 +573,20 @@ __device__ __forceinline__ unsigned long long is_walk_blocks(
       if (i + 1ull < nblk) nx = v6_ldg(is_block_move<kStride>(rows, dig, b + 1ull));
     }
     // digit 1 runs up through block b when b is even
+    int bm = 0;
     if ((b & 1ull) == 0ull) {
-      TG_IS_SWEEP(0); TG_IS_MOVE(0); TG_IS_SWEEP(1); TG_IS_MOVE(1); TG_IS_SWEEP(2);
-      TG_IS_MOVE(2); TG_IS_SWEEP(3); TG_IS_MOVE(3); TG_IS_SWEEP(4); TG_IS_MOVE(4);
-      TG_IS_SWEEP(5); TG_IS_MOVE(5); TG_IS_SWEEP(6);
+      TG_IS_SWEEP; TG_IS_MOVE(0); TG_IS_SWEEP; TG_IS_MOVE(1); TG_IS_SWEEP; TG_IS_MOVE(2);
+      TG_IS_SWEEP; TG_IS_MOVE(3); TG_IS_SWEEP; TG_IS_MOVE(4); TG_IS_SWEEP; TG_IS_MOVE(5);
+      TG_IS_SWEEP;
     } else {
-      TG_IS_SWEEP(6); TG_IS_MOVE(5); TG_IS_SWEEP(5); TG_IS_MOVE(4); TG_IS_SWEEP(4);
-      TG_IS_MOVE(3); TG_IS_SWEEP(3); TG_IS_MOVE(2); TG_IS_SWEEP(2); TG_IS_MOVE(1);
-      TG_IS_SWEEP(1); TG_IS_MOVE(0); TG_IS_SWEEP(0);
+      TG_IS_SWEEP; TG_IS_MOVE(5); TG_IS_SWEEP; TG_IS_MOVE(4); TG_IS_SWEEP; TG_IS_MOVE(3);
+      TG_IS_SWEEP; TG_IS_MOVE(2); TG_IS_SWEEP; TG_IS_MOVE(1); TG_IS_SWEEP; TG_IS_MOVE(0);
+      TG_IS_SWEEP;
     }
+    // The high columns hold the set's pivot columns, where a codeword equals
+    // its message, so they weigh at least hb: only a block whose lightest low
+    // half plus hb is below wmin can lower it, and is counted exactly.
+    if (32 - bm + hb < wmin) wmin = is_block_exact<kStride>(rows, r0, r1, rc, dig, n_dig, b, wmin);
     if (wmin < wthr) break;
     if ((i & 15ull) == 15ull && ld_flag(stop)) break;
   }
