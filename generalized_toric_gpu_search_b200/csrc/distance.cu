@@ -889,11 +889,12 @@ int run_walk(const DistArgs& args, int sm_count, int blocks_per_sm, int tpb, cud
   }
   if (e != cudaSuccess) return cuda_fail(e, "walk kernel launch");
   if ((parts & kWalkInfoset) && args.is_min_k <= args.k_max) {
-    // Information-set walk, one level per launch triple; 512 resident
-    // threads per SM (128 registers).  Levels no code needs find no tasks.
-    constexpr int kPerSm = 512 / kIsWalkThreads;
+    // Information-set walk, one level per launch triple; 6 CTAs of 128
+    // threads per SM (80 registers, 27 KB of shared memory each).  Levels no
+    // code needs find no tasks.
+    constexpr int kPerSm = 6;
     DistArgs la = args;
-    la.is_lanes = sm_count * 512;
+    la.is_lanes = sm_count * kPerSm * kIsWalkThreads;
     const int plan_grid = (args.n + 255) / 256;
     for (int w = 1; w <= args.k_max; ++w) {
       plan_level_kernel<<<plan_grid, 256, 0, s>>>(la, w);

@@ -532,31 +532,42 @@ __device__ __noinline__ int is_block_exact(const V6* rows, uint32_t r0, uint32_t
     bm = __vimax3_s32(bm, __vimax3_s32(z0_, z1_, z2_) + zz_,                                     \
                       __vimax3_s32(z3_, z4_, max(z5_, z6_)) + zz_);                      \
   }
-#define TG_IS_MOVE(I) \
-  pl3_xor(W, E[I]);   \
-  pl3_xor(Pz, Z[I])
+#define TG_IS_MOVE(I)                                                        \
+  {                                                                          \
+    W.x0 ^= ez[(6 * (I) + 0) * kStride];                                     \
+    W.x1 ^= ez[(6 * (I) + 1) * kStride];                                     \
+    W.x2 ^= ez[(6 * (I) + 2) * kStride];                                     \
+    Pz.x0 ^= ez[(6 * (I) + 3) * kStride];                                    \
+    Pz.x1 ^= ez[(6 * (I) + 4) * kStride];                                    \
+    Pz.x2 ^= ez[(6 * (I) + 5) * kStride];                                    \
+  }
 
 // Walks blocks [b0, b0 + nblk) of one support; P is the sum of its rows other
 // than digit 0 at the start of block b0.  Each block is 7 sweeps of digit 0
 // (row r0) with digit 1 (row r1) moving between them: 49 codewords of
-// straight-line code with digit 1's six moves in registers.  The move between
-// blocks (digits 2.., rows dig[]) is loaded a block ahead.  Returns the
-// codewords evaluated.
+// straight-line code.  Digit 1's six moves, in the W domain and on g's zero
+// columns, are kept in this thread's shared-memory slots ez (stride kStride);
+// the move between blocks (digits 2.., rows dig[]) is loaded a block ahead.
+// Returns the codewords evaluated.
 template <int kStride>
 __device__ __forceinline__ unsigned long long is_walk_blocks(
     const V6& P, const V6* rows, uint32_t r0, uint32_t r1, uint32_t rc, const uint16_t* dig,
-    int n_dig, unsigned long long b0, unsigned long long nblk, int hb, int wthr,
+    uint32_t* ez, int n_dig, unsigned long long b0, unsigned long long nblk, int hb, int wthr,
     const int32_t* stop, int& wmin) {
   const Pl3 g = pl3_lo(v6_ldg(rows + r0));
   const Pl3 h = pl3_inv(g);
   const uint32_t gz = ~(g.x0 | g.x1 | g.x2);  // low columns where g is 0
   const int ngz = __popc(gz);
-  Pl3 E[6], Z[6];
 #pragma unroll
   for (int i = 0; i < 6; ++i) {
     const Pl3 d = pl3_lo(v6_ldg(rows + r1 + 1 + i));
-    E[i] = pl3_mul(d, h);
-    Z[i] = pl3_and(d, gz);
+    const Pl3 e = pl3_mul(d, h);
+    ez[(6 * i + 0) * kStride] = e.x0;
+    ez[(6 * i + 1) * kStride] = e.x1;
+    ez[(6 * i + 2) * kStride] = e.x2;
+    ez[(6 * i + 3) * kStride] = d.x0 & gz;
+    ez[(6 * i + 4) * kStride] = d.x1 & gz;
+    ez[(6 * i + 5) * kStride] = d.x2 & gz;
   }
   Pl3 W = pl3_mul(pl3_lo(P), h);
   Pl3 Pz = pl3_and(pl3_lo(P), gz);
@@ -598,12 +609,12 @@ __device__ __forceinline__ unsigned long long is_walk_blocks(
 
 // Units [u0, u1) of code c at level w (flat over set, support, block); the
 // smallest weight met (or wmin when none is smaller), and the codewords
-// evaluated in ncw.  dig (stride kStride) is this thread's scratch for the
-// rows of digits 2..w-2.
+// evaluated in ncw.  dig and ez (stride kStride) are this thread's shared
+// scratch: the rows of digits 2..w-2 and digit 1's moves.
 template <int kStride>
 __device__ __forceinline__ int is_walk_units(const DistArgs& a,
                                              const unsigned long long (*bn)[kIsBinom],
-                                             uint16_t* dig, int c, int k, int w,
+                                             uint16_t* dig, uint32_t* ez, int c, int k, int w,
                                              unsigned long long u0, unsigned long long u1,
                                              int wthr, int wmin, unsigned long long& ncw) {
   const unsigned long long n_sup = bn[k][w];
@@ -672,7 +683,7 @@ __device__ __forceinline__ int is_walk_units(const DistArgs& a,
       // that do not fit in the 17 high columns (k > 17).
       const int dj = int(j) == n_sets - 1 ? delta : 0;
       const int hb = max(0, w - dj - max(0, (k - dj) - 17));
-      ncw += is_walk_blocks<kStride>(P, rows, r0, r1, rc, dig, w - 3, b, nblk, hb, wthr, stop,
+      ncw += is_walk_blocks<kStride>(P, rows, r0, r1, rc, dig, ez, w - 3, b, nblk, hb, wthr, stop,
                                      wmin);
     }
     u += nblk;
@@ -687,6 +698,7 @@ template <int kTPB, int kMinBlocks>
 __global__ void __launch_bounds__(kTPB, kMinBlocks) walk_level_kernel(DistArgs a, int w) {
   __shared__ unsigned long long s_binom[kIsBinom][kIsBinom];
   __shared__ uint16_t s_dig[kIsMaxDigits][kTPB];
+  __shared__ uint32_t s_ez[36][kTPB];
   for (int i = threadIdx.x; i < kIsBinom * kIsBinom; i += kTPB)
     s_binom[i / kIsBinom][i % kIsBinom] = c_binom[i / kIsBinom][i % kIsBinom];
   __syncthreads();
@@ -695,6 +707,7 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) walk_level_kernel(DistArgs a
   const unsigned long long nb = a.is_hdr->units;
   unsigned long long evaluated = 0ull;
   uint16_t* my_dig = &s_dig[0][threadIdx.x];  // this thread's digit rows, stride kTPB
+  uint32_t* my_ez = &s_ez[0][threadIdx.x];     // this thread's digit-1 moves, stride kTPB
   for (;;) {
     unsigned long long base = 0ull;
     if (lane == 0) base = atomicAdd(&a.is_hdr->counter, 32ull);
@@ -717,7 +730,7 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) walk_level_kernel(DistArgs a
     unsigned long long ncw = 0ull;
     // Codewords no lighter than the code's best so far cannot change it, so
     // the walk starts from that best.
-    const int wmin = is_walk_units<kTPB>(a, s_binom, my_dig, c, a.desc[c].k, w, u0, u1, wthr,
+    const int wmin = is_walk_units<kTPB>(a, s_binom, my_dig, my_ez, c, a.desc[c].k, w, u0, u1, wthr,
                                          ld_flag(a.is_best + c), ncw);
     evaluated += ncw;
     const int best = min(atomicMin(a.is_best + c, wmin), wmin);
