@@ -45,10 +45,22 @@ POPC_PER_CODEWORD = 14.0 / 8.0  # histogram walk: 7 bins x 2 words per 8 codewor
 POPC_PER_CODEWORD_INFOSET = 8.0 / 7.0
 
 
-def launches_per_step(k_max: int) -> int:
-    """Kernels per step: prep_exact, prep_infoset, scan_tasks, walk_hist, then
-    per information-set level plan, scan and walk, and finalize_infoset."""
-    return 5 + 3 * k_max
+# --enumeration: (TG_ENUM_* value, description)
+ENUMERATIONS = {
+    "auto": (0, "auto: information sets for k >= 10, orbit (projective + torus "
+                "normalisation) below"),
+    "projective": (1, "projective messages"),
+    "orbit": (2, "orbit (projective + torus normalisation)"),
+    "infoset": (3, "information sets for every set"),
+}
+
+
+def launches_per_step(k_max: int, enumeration: str) -> int:
+    """Kernels per step: prep_exact, scan_tasks and the enumeration walk; with
+    information sets also prep_infoset, per level plan, scan and walk, and
+    finalize_infoset."""
+    infoset = enumeration == "infoset" or (enumeration == "auto" and k_max >= 10)
+    return 3 + ((2 + 3 * k_max) if infoset else 0)
 L2_FLUSH_BYTES = 256 << 20
 
 
@@ -355,10 +367,12 @@ def mutation_stream(n: int, seed: int, k_lo: int = 10, k_hi: int = 15):
     return out
 
 
-def bench_served(dev: int, n: int = 3000, rate: float = 300.0) -> dict:
+def bench_served(dev: int, n: int = 3000, rate: float = 300.0, engine: str = "batch") -> dict:
     """Served search stream: Poisson arrivals at `rate` per second of mutated
-    candidates, each with the running best-known d of its k as threshold."""
-    from generalized_toric_gpu_search_b200.serve import ToricServer
+    candidates, each with the running best-known d of its k as threshold.
+    engine "batch": ToricBatchServer (continuous micro-batches of the batch
+    path); "persistent": ToricServer (the device-resident request loop)."""
+    from generalized_toric_gpu_search_b200.serve import ToricBatchServer, ToricServer
 
     stream = mutation_stream(n, BASE_SEED + 7)
     rng = np.random.default_rng(BASE_SEED + 11)
@@ -375,7 +389,9 @@ def bench_served(dev: int, n: int = 3000, rate: float = 300.0) -> dict:
                 if a.min_distance > best[k]:
                     best[k] = a.min_distance
 
-    with ToricServer(dev, k_max=15) as srv:
+    make = (lambda: ToricBatchServer(dev, k_max=15)) if engine == "batch" else \
+        (lambda: ToricServer(dev, k_max=15))
+    with make() as srv:
         srv.evaluate([(s, best[len(s)]) for s in stream[:32]])  # warm the loop
         futs = []
         t0 = time.perf_counter()
@@ -392,7 +408,7 @@ def bench_served(dev: int, n: int = 3000, rate: float = 300.0) -> dict:
         answers = [f.result(timeout=600) for f in futs]
         total = time.perf_counter() - t0
         st = srv.stats()
-        slots = srv.slots
+        slots = getattr(srv, "slots", None)
         # Saturation: a second stream of the same size submitted at once.
         burst = mutation_stream(n, BASE_SEED + 13)
         tb = time.perf_counter()
@@ -402,13 +418,15 @@ def bench_served(dev: int, n: int = 3000, rate: float = 300.0) -> dict:
     dev_t = np.array([a.device_s for a in answers])
     return {"workload": (f"{n:,} Poisson arrivals at {rate:.0f}/s, single mutations of 256 seeded "
                          "parents, |P| 10..15, td = running best-known d per k"),
+            "engine": engine,
             "codes_per_s": n / total, "seconds": total,
             "p50_ms": 1e3 * float(np.percentile(lat, 50)),
             "p99_ms": 1e3 * float(np.percentile(lat, 99)),
             "device_p50_ms": 1e3 * float(np.percentile(dev_t, 50)),
             "device_p99_ms": 1e3 * float(np.percentile(dev_t, 99)),
             "dedup_answers": st["dedup_answers"], "passed": int(sum(a.passed for a in answers)),
-            "slots": slots, "loop_launches": st["loop_launches"],
+            "slots": slots, "loop_launches": st.get("loop_launches"),
+            "batches": st.get("batches"),
             "burst_codes_per_s": n / burst_s,
             "best_known_d_end": best}
 
@@ -457,7 +475,8 @@ def run_b200_arm(args, d: Dist) -> None:
     sets = make_workload(d.rank, args.n_sets, args.kmin, args.kmax)
     M = build_eval_matrix()
     ctx = ToricContext(dev, M)
-    cfg = LaunchConfig(tail_rows=args.tail_rows, blocks_per_sm=args.blocks_per_sm)
+    cfg = LaunchConfig(tail_rows=args.tail_rows, blocks_per_sm=args.blocks_per_sm,
+                       enumeration=ENUMERATIONS[args.enumeration][0])
     runner = DistanceRunner(ctx, cfg)
     flat, offsets, kmax = pack_sets(sets)
     d_idx = torch.from_numpy(flat).to(device)
@@ -590,7 +609,8 @@ def run_b200_arm(args, d: Dist) -> None:
     if d.rank == 0 and not args.skip_extra:
         extra["canonical_forms"] = bench_canonical(dev)
         extra["early_exit_k15"] = bench_early_exit(dev)
-        extra["served_stream"] = bench_served(dev)
+        extra["served_stream"] = bench_served(dev, engine="batch")
+        extra["served_stream_persistent"] = bench_served(dev, engine="persistent")
 
     cpu = None
     if d.rank == 0 and d.world == 1 and not args.skip_cpu:
@@ -605,8 +625,7 @@ def run_b200_arm(args, d: Dist) -> None:
             "data": "synthetic (seeded random exponent sets)",
             "config": {"workload": WORKLOAD, "n_sets_per_gpu": len(sets),
                        "k_range": [K_LO, K_HI], "target_distance": 1,
-                       "enumeration": "auto: information sets for k >= 10, orbit "
-                                      "(projective + torus normalisation) below",
+                       "enumeration": ENUMERATIONS[args.enumeration][1],
                        "variant": "histogram", "tail_rows": args.tail_rows or 4,
                        "launch": "CUDA graphs: prepare, enumeration walk, information-set walk",
                        "l2": "256 MiB write between timed steps",
@@ -619,7 +638,7 @@ def run_b200_arm(args, d: Dist) -> None:
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * e2e_max / args.steps,
                     "api": "DistanceOracleCUDABP.max_zeros_batch(list of lists, 1)"},
-            "gpu_launches": launches_per_step(kmax) * args.steps,
+            "gpu_launches": launches_per_step(kmax, args.enumeration) * args.steps,
             "roofline": {"bound": "int (POPC pipe)", "achieved": achieved / 1e12,
                          "peak": peak / 1e12, "unit": "Tpopc/s", "frac": achieved / peak,
                          "traffic": None, "kernel": dominant["kernel"],
@@ -646,6 +665,8 @@ def main(argv=None) -> None:
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--tail-rows", type=int, default=0)
     ap.add_argument("--blocks-per-sm", type=int, default=0)
+    ap.add_argument("--enumeration", choices=sorted(ENUMERATIONS), default="auto",
+                    help="exact enumeration of the headline workload")
     ap.add_argument("--skip-plain", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-extra", action="store_true",
@@ -653,7 +674,7 @@ def main(argv=None) -> None:
     ap.add_argument("--n-sets", type=int, default=N_SETS, help="sets per GPU (small cases)")
     ap.add_argument("--kmin", type=int, default=K_LO)
     ap.add_argument("--kmax", type=int, default=K_HI)
-    ap.add_argument("--section", choices=["canonical", "early-exit", "served"],
+    ap.add_argument("--section", choices=["canonical", "early-exit", "served", "served-persistent"],
                     help="run one secondary configuration alone and print its JSON")
     ap.add_argument("--canon-n", type=int, default=1_000_000)
     args = ap.parse_args(argv)
@@ -664,7 +685,8 @@ def main(argv=None) -> None:
         lib_build.build()
         fn = {"canonical": lambda: bench_canonical(0, args.canon_n),
               "early-exit": lambda: bench_early_exit(0),
-              "served": lambda: bench_served(0)}[args.section]
+              "served": lambda: bench_served(0, engine="batch"),
+              "served-persistent": lambda: bench_served(0, engine="persistent")}[args.section]
         print(json.dumps({"section": args.section, **fn()}), flush=True)
         return
     if args.impl == "reference":

@@ -217,3 +217,216 @@ class ToricServer:
             for f in waiters:
                 if not f.done():
                     f.set_exception(exc)
+
+
+class ToricBatchServer:
+    """max_zeros requests served as continuous micro-batches of the batch path.
+
+    A worker thread takes every request waiting when the GPU becomes free and
+    runs them as one tg_max_zeros batch (information sets for k >= 10, one
+    launch per level, so a batch of any size costs about the same fixed
+    launch overhead plus its work).  Requests that arrive meanwhile form the
+    next batch.  Canonical dedup as in ToricServer: the AGL2(F7) canonical
+    mask keys a host cache of earlier answers, a request is answered from it
+    when the cached answer decides its threshold (an exact value, or a failure
+    witness at a threshold no larger than this one), and equivalent requests
+    of one batch share one evaluation at their smallest threshold, which
+    decides all of them.  Answers follow the batch oracle's contract: `passed`
+    (max_zeros <= 49 - td, value exact) or a failure witness above 49 - td.
+    """
+
+    def __init__(self, device_id: int = 0, M: np.ndarray | None = None, *, k_max: int = 21,
+                 max_batch: int = 1 << 16, dedup: bool = True, cache_size: int = 1 << 20):
+        from .distance import MAX_EXACT_K, DistanceRunner, LaunchConfig
+
+        if not 0 <= k_max <= MAX_EXACT_K:
+            raise ValueError("k_max must lie in 0..21")
+        self.ctx = ToricContext(device_id, build_eval_matrix() if M is None else M)
+        self.device = torch.device("cuda", device_id)
+        self.k_max = k_max
+        self.max_batch = max_batch
+        self.dedup = dedup
+        self.cache_size = cache_size
+        self._lib = _lib.load()
+        self._runner = DistanceRunner(self.ctx, LaunchConfig())
+        self._stream = torch.cuda.Stream(device=self.device)
+        self._cache: dict[int, tuple[int, int]] = {}  # canonical mask -> (max_zeros, td)
+        self._cv = threading.Condition()
+        self._pending: deque = deque()
+        self._closed = False
+        self._error: BaseException | None = None
+        self._next_id = 0
+        self._stats = {"published": 0, "finished": 0, "batches": 0, "evaluated": 0,
+                       "dedup_answers": 0, "codewords": 0}
+        self._thread = threading.Thread(target=self._loop, name="toric-batch-server",
+                                        daemon=True)
+        self._thread.start()
+
+    # -- client API -----------------------------------------------------------
+
+    def submit(self, indices, target_distance: int) -> Future:
+        """Queues one request; the future yields a ServeAnswer."""
+        idx = np.ascontiguousarray(np.asarray(indices, dtype=np.int32).reshape(-1))
+        if idx.size > self.k_max:
+            raise ValueError(f"request has k = {idx.size} > k_max = {self.k_max}")
+        if idx.size and (int(idx.min()) < 0 or int(idx.max()) >= N_POINTS):
+            raise ValueError("exponent indices must lie in 0..48")
+        fut: Future = Future()
+        with self._cv:
+            if self._closed:
+                raise RuntimeError("server is closed")
+            if self._error is not None:
+                raise RuntimeError("server failed") from self._error
+            rid = self._next_id
+            self._next_id += 1
+            self._pending.append((rid, idx, int(target_distance), fut, time.perf_counter()))
+            self._stats["published"] += 1
+            self._cv.notify()
+        return fut
+
+    def evaluate(self, requests, timeout: float = 600.0) -> list[ServeAnswer]:
+        """Submits (indices, target_distance) pairs and waits for all answers."""
+        futs = [self.submit(s, td) for s, td in requests]
+        return [f.result(timeout=timeout) for f in futs]
+
+    def stats(self) -> dict:
+        with self._cv:
+            out = dict(self._stats)
+            out["outstanding"] = out["published"] - out["finished"]
+        return out
+
+    def close(self) -> None:
+        with self._cv:
+            if self._closed:
+                return
+            self._closed = True
+            self._cv.notify()
+        self._thread.join(timeout=60)
+        self.ctx.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- worker ---------------------------------------------------------------
+
+    def _loop(self) -> None:
+        while True:
+            with self._cv:
+                while not self._pending and not self._closed:
+                    self._cv.wait(timeout=0.05)
+                if not self._pending and self._closed:
+                    return
+                batch = [self._pending.popleft()
+                         for _ in range(min(len(self._pending), self.max_batch))]
+            try:
+                self._serve(batch)
+            except BaseException as exc:  # noqa: BLE001 - surfaced to every waiter
+                with self._cv:
+                    self._error = exc
+                    rest = list(self._pending)
+                    self._pending.clear()
+                for item in batch + rest:
+                    if not item[3].done():
+                        item[3].set_exception(exc)
+                return
+
+    def _canonical(self, masks: np.ndarray) -> np.ndarray:
+        n = masks.shape[0]
+        s = self._stream
+        with torch.cuda.device(self.device), torch.cuda.stream(s):
+            d_in = torch.from_numpy(masks.view(np.int64)).pin_memory().to(self.device,
+                                                                          non_blocking=True)
+            out = torch.empty(n, dtype=torch.int64, device=self.device)
+            _lib.check(self._lib.tg_canonical_masks(self.ctx.handle, d_in.data_ptr(), n,
+                                                    out.data_ptr(), None, None, s.cuda_stream),
+                       "tg_canonical_masks")
+            h = torch.empty(n, dtype=torch.int64, pin_memory=True)
+            h.copy_(out, non_blocking=True)
+        s.synchronize()
+        return h.numpy().view(np.uint64).copy()
+
+    def _run(self, sets: list[np.ndarray], tds: list[int]) -> tuple[list[int], float]:
+        from .distance import pack_sets
+
+        flat, offsets, k_max = pack_sets(sets)
+        n = len(sets)
+        s = self._stream
+        runner = self._runner
+        with torch.cuda.device(self.device), torch.cuda.stream(s):
+            d_idx = torch.from_numpy(flat if flat.size else np.zeros(1, np.int32)).pin_memory()
+            d_idx = d_idx.to(self.device, non_blocking=True)
+            d_off = torch.from_numpy(offsets).pin_memory().to(self.device, non_blocking=True)
+            d_td = torch.from_numpy(np.asarray(tds, dtype=np.int32)).pin_memory().to(
+                self.device, non_blocking=True)
+            d_out = torch.empty(n, dtype=torch.int32, device=self.device)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            p = runner.params(n, max(k_max, 1), 0)
+            e0.record(s)
+            runner.run(p, d_idx, d_off, d_out, d_target=d_td, stream=s)
+            e1.record(s)
+            h_out = torch.empty(n, dtype=torch.int32, pin_memory=True)
+            h_out.copy_(d_out, non_blocking=True)
+        status = runner.status(p, s)  # synchronises the stream
+        if status != _lib.TG_OK:
+            _lib.check(status, "served batch (device)")
+        _, cw, _ = runner.counters(s)
+        with self._cv:
+            self._stats["codewords"] += cw
+        return h_out.tolist(), e0.elapsed_time(e1) / 1e3
+
+    def _serve(self, batch) -> None:
+        n = len(batch)
+        keys: list[int | None] = [None] * n
+        if self.dedup:
+            masks = np.zeros(n, dtype=np.uint64)
+            ok = np.zeros(n, dtype=bool)
+            for i, (_, idx, _, _, _) in enumerate(batch):
+                if idx.size >= 1 and np.unique(idx).size == idx.size:
+                    masks[i] = np.uint64(int(np.bitwise_or.reduce(
+                        np.left_shift(np.uint64(1), idx.astype(np.uint64)))))
+                    ok[i] = True
+            if ok.any():
+                canon = self._canonical(masks[ok])
+                for i, c in zip(np.flatnonzero(ok), canon.tolist()):
+                    keys[i] = int(c)
+        answers: list[tuple[int, bool] | None] = [None] * n  # (max_zeros, dedup)
+        groups: dict = {}
+        for i, (_, idx, td, _, _) in enumerate(batch):
+            key = keys[i]
+            if key is not None and key in self._cache:
+                mz, td_c = self._cache[key]
+                if mz <= N_POINTS - td_c or td >= td_c:
+                    answers[i] = (mz, True)
+                    continue
+            groups.setdefault(key if key is not None else ("solo", i), []).append(i)
+        reps = list(groups.values())
+        device_s = 0.0
+        if reps:
+            sets = [batch[g[0]][1] for g in reps]
+            tds = [min(batch[i][2] for i in g) for g in reps]
+            values, device_s = self._run(sets, tds)
+            for g, mz, td in zip(reps, values, tds):
+                key = keys[g[0]]
+                if key is not None:
+                    old = self._cache.get(key)
+                    exact = mz <= N_POINTS - td
+                    if old is None or exact or td < old[1]:
+                        if len(self._cache) >= self.cache_size:
+                            self._cache.clear()
+                        self._cache[key] = (mz, td)
+                for j, i in enumerate(g):
+                    answers[i] = (mz, j > 0)
+        now = time.perf_counter()
+        n_dedup = sum(1 for a in answers if a[1])
+        with self._cv:
+            self._stats["batches"] += 1
+            self._stats["evaluated"] += len(reps)
+            self._stats["dedup_answers"] += n_dedup
+            self._stats["finished"] += n
+        for (rid, idx, td, fut, t0), (mz, dd) in zip(batch, answers):
+            fut.set_result(ServeAnswer(id=rid, max_zeros=int(mz),
+                                       passed=bool(mz <= N_POINTS - td), dedup=dd,
+                                       latency_s=now - t0, device_s=device_s))
