@@ -398,8 +398,13 @@ def bench_served(dev: int, n: int = 3000, rate: float = 300.0, engine: str = "ba
         t_next = t0
         for s, gap in zip(stream, gaps):
             t_next += gap
-            while time.perf_counter() < t_next:
-                pass
+            # Sleep (which releases the GIL for the server's threads) rather
+            # than spin until the arrival time.
+            while True:
+                wait = t_next - time.perf_counter()
+                if wait <= 0.0:
+                    break
+                time.sleep(wait)
             with lock:
                 td = best[len(s)]
             f = srv.submit(s, td)
