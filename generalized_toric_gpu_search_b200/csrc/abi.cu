@@ -299,6 +299,7 @@ static int bind_distance(tg_context* ctx, const tg_distance_params* p, const int
   a.seed = p->sample_seed;
   a.tab.M = ctx->d_M;
   a.tab.gl2 = ctx->d_gl2;
+  a.is_toric = ctx->is_toric;
   bind_workspace(a, L, d_workspace);
   return TG_OK;
 }

@@ -92,6 +92,7 @@ struct DistArgs {
   int bitpat_stride;
   // Information-set path: codes with is_min_k <= k (is_min_k > k_max: none).
   int is_min_k;
+  int is_toric;                  // M is the toric matrix (torus translations are automorphisms)
   int is_stride;                 // V6 per code in is_rows
   int is_lanes;                  // resident threads of the walk (task sizing)
   IsHeader* is_hdr;              // task queue of the information-set walk

@@ -168,6 +168,60 @@ __device__ __forceinline__ void is_reorder_columns(uint64_t piv, uint64_t& p0, u
   p2 = q2;
 }
 
+// Discrete logarithms of the field elements 1..7 (alpha = x; index 0 unused)
+// and inverses modulo 7.
+__constant__ uint8_t c_alpha_log[8] = {0, 0, 1, 3, 2, 6, 4, 5};
+__constant__ uint8_t c_inv7[7] = {0, 1, 4, 5, 2, 3, 6};
+
+// The columns of try t's random affine image E1 = A T + s of the k-point
+// tile (e1), and of its translates A (T + t_i) + s = E1 + A t_i (cover).
+// Column j is the torus point (1 + j / 7, 1 + j % 7), i.e. (alpha^a, alpha^b)
+// with (a, b) its logarithms.  A is invertible, so the translates stay
+// pairwise disjoint, and E1 + A t_i is a torus translate of E1.
+__device__ void is_tile_image(int lane, int k, int m_t, int t, uint64_t& e1, uint64_t& cover) {
+  uint64_t sd = splitmix64(0xC6A4A7935BD1E995ull + uint64_t(t) * 0x9E3779B97F4A7C15ull);
+  int p, q, r, s, det;
+  do {
+    p = int(sd % 7ull);
+    sd = splitmix64(sd);
+    q = int(sd % 7ull);
+    sd = splitmix64(sd);
+    r = int(sd % 7ull);
+    sd = splitmix64(sd);
+    s = int(sd % 7ull);
+    sd = splitmix64(sd);
+    det = ((p * s - q * r) % 7 + 7) % 7;
+  } while (det == 0);
+  const int u = int(sd % 7ull);
+  sd = splitmix64(sd);
+  const int v = int(sd % 7ull);
+  const int di = c_inv7[det];  // A^-1 = det^-1 (s, -q; -r, p)
+  const int i00 = (s * di) % 7, i01 = ((7 - q) * di) % 7;
+  const int i10 = ((7 - r) * di) % 7, i11 = (p * di) % 7;
+  const uint64_t tile = c_tile_mask[k];
+  bool in_e1[2] = {false, false}, in_cov[2] = {false, false};
+#pragma unroll
+  for (int half = 0; half < 2; ++half) {
+    const int col = lane + 32 * half;
+    if (col >= kN) continue;
+    const int da = (c_alpha_log[1 + col / 7] - u + 7) % 7;
+    const int db = (c_alpha_log[1 + col % 7] - v + 7) % 7;
+    const int za = (i00 * da + i01 * db) % 7, zb = (i10 * da + i11 * db) % 7;
+    for (int i = 0; i < m_t; ++i) {
+      const int ta = (za - c_tile_shift[k][i][0] + 7) % 7;
+      const int tb = (zb - c_tile_shift[k][i][1] + 7) % 7;
+      if ((tile >> (ta * 7 + tb)) & 1ull) {
+        in_cov[half] = true;
+        if (i == 0) in_e1[half] = true;
+      }
+    }
+  }
+  e1 = uint64_t(__ballot_sync(0xffffffffu, in_e1[0])) |
+       (uint64_t(__ballot_sync(0xffffffffu, in_e1[1])) << 32);
+  cover = uint64_t(__ballot_sync(0xffffffffu, in_cov[0])) |
+          (uint64_t(__ballot_sync(0xffffffffu, in_cov[1])) << 32);
+}
+
 // Writes the rows of one set: g and the six Gray-step deltas per row.
 __device__ __forceinline__ void is_store_set(V6* dst, int lane, int k, uint64_t p0, uint64_t p1,
                                              uint64_t p2) {
@@ -238,8 +292,70 @@ __global__ void __launch_bounds__(kIsPrepWarps * 32) prep_infoset_kernel(DistArg
     }
     if (best_score >= ideal) break;
   }
+  // Plan "translates" (toric M): one information set E1 whose torus
+  // translates are disjoint covers as many sets as it has translates, all
+  // enumerated by E1 alone (a translate's codewords are shifted codewords of
+  // E1's, with the same weights); a second set E2 on the leftover columns
+  // adds one more when it has full rank (or a partial one).  It replaces the
+  // plan above when its bound is at least as large at every level and it
+  // enumerates no more sets.
+  const int m_b = best_score >= 0 ? best_score / 64 : 0;
+  const int r_b = best_score >= 0 ? best_score % 64 : 0;
+  const int delta_b = (r_b > 0 && k - r_b <= kIsMaxDelta && m_b < cap_sets) ? k - r_b : 0;
+  bool use_t = false;
+  uint64_t t_e1 = 0ull, t_left = 0ull;
+  int t_full = 0, t_delta = 0;
+  bool t_e2 = false;
+  if (a.is_toric && !deficient && c_tile_m[k] >= 1) {
+    is_make_order(s_ord[wl], 0, lane);  // identity order; `used` masks select the columns
+    const int m_t = c_tile_m[k];
+    for (int t = 0; t < kIsTries && t_e1 == 0ull; ++t) {
+      uint64_t e1 = 0ull, cover = 0ull;
+      is_tile_image(lane, k, m_t, t, e1, cover);
+      uint64_t p0 = o0, p1 = o1, p2 = o2, used = ~e1 & kMask49;
+      if (is_gauss_jordan(lane, k, p0, p1, p2, used, s_ord[wl]) == k) {
+        t_e1 = e1;
+        t_left = ~cover & kMask49;
+      }
+    }
+    if (t_e1 != 0ull) {
+      uint64_t p0 = o0, p1 = o1, p2 = o2, used = ~t_left & kMask49;
+      const int r2 = t_left ? is_gauss_jordan(lane, k, p0, p1, p2, used, s_ord[wl]) : 0;
+      t_full = m_t + (r2 == k ? 1 : 0);
+      t_delta = (r2 > 0 && r2 < k && k - r2 <= kIsMaxDelta) ? k - r2 : 0;
+      t_e2 = r2 == k || t_delta > 0;
+      const int cost_t = 1 + (t_e2 ? 1 : 0);
+      const int cost_b = m_b + (delta_b > 0 ? 1 : 0);
+      bool dominates = cost_t <= cost_b;
+      for (int L = 0; L <= k && dominates; ++L) {
+        const int f_t = t_full * (L + 1) + (t_delta > 0 ? max(0, L + 1 - t_delta) : 0);
+        const int f_b = m_b * (L + 1) + (delta_b > 0 ? max(0, L + 1 - delta_b) : 0);
+        dominates = f_t >= f_b;
+      }
+      use_t = dominates;
+    }
+  }
   int n_sets = 0, m_full = 0, delta = 0;
-  if (!deficient) {
+  if (use_t) {
+    V6* base = a.is_rows + size_t(c) * a.is_stride;
+    uint64_t p0 = o0, p1 = o1, p2 = o2, used = ~t_e1 & kMask49;
+    is_gauss_jordan(lane, k, p0, p1, p2, used, s_ord[wl]);
+    is_reorder_columns(t_e1, p0, p1, p2);
+    is_store_set(base, lane, k, p0, p1, p2);
+    n_sets = 1;
+    if (t_e2) {
+      p0 = o0;
+      p1 = o1;
+      p2 = o2;
+      used = ~t_left & kMask49;
+      is_gauss_jordan(lane, k, p0, p1, p2, used, s_ord[wl]);
+      is_reorder_columns(used & t_left, p0, p1, p2);
+      is_store_set(base + size_t(k) * kIsVecPerRow, lane, k, p0, p1, p2);
+      n_sets = 2;
+    }
+    m_full = t_full;
+    delta = t_delta;
+  } else if (!deficient) {
     is_make_order(s_ord[wl], best_t, lane);
     uint64_t p0 = o0, p1 = o1, p2 = o2, used = 0ull;
     V6* base = a.is_rows + size_t(c) * a.is_stride;
