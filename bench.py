@@ -167,7 +167,7 @@ class ClockSampler:
             os.close(fd)
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu_index}", f"--query-gpu={self.QUERY}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "20"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
@@ -598,7 +598,8 @@ def run_b200_arm(args, d: Dist) -> None:
     peak = pipes.get("popc_per_clk_sm", 16.0) * sm_count * (mhz or 1965.0) * 1e6
     enum_s, is_s = statistics.mean(enum_ms) / 1e3, statistics.mean(is_ms) / 1e3
     if is_s >= enum_s:
-        dominant = {"kernel": "walk_infoset_kernel (+ finalize_infoset_kernel)",
+        dominant = {"kernel": "walk_level_kernel (one launch per level, with plan_level_kernel, "
+                              "scan_level_kernel and finalize_infoset_kernel)",
                     "seconds": is_s, "codewords": paths["infoset_codewords"],
                     "popc_per_codeword": POPC_PER_CODEWORD_INFOSET,
                     "note": "8 POPC per 7 codewords (seven zero-selection counts on the low "
@@ -665,7 +666,7 @@ def run_b200_arm(args, d: Dist) -> None:
 def main(argv=None) -> None:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--tail-rows", type=int, default=0)
