@@ -466,7 +466,22 @@ __global__ void __launch_bounds__(kScanThreads) scan_level_kernel(DistArgs a, in
     }
     const unsigned long long target = 8ull * static_cast<unsigned long long>(a.is_lanes);
     unsigned long long nb = (tot + target - 1ull) / target;
-    s_nb = max(1ull, min(nb, is_max_task_units(w)));
+    nb = max(1ull, min(nb, is_max_task_units(w)));
+    // Align tasks with supports (units per support is a power of 7): whole
+    // supports, or the power of 7 dividing one that is nearest on a log
+    // scale, so the lanes of a warp walk equal block counts.
+    const unsigned long long bps = is_units_per_support(w);
+    if (bps > 1ull) {
+      if (nb >= bps) {
+        nb = (nb / bps) * bps;
+      } else {
+        unsigned long long p7 = 1ull;
+        while (p7 * 7ull <= nb) p7 *= 7ull;
+        // 7 p7 when nb > sqrt(7) p7 (nb^2 > 7 p7^2); 7 p7 <= bps here
+        nb = (nb * nb > 7ull * p7 * p7) ? 7ull * p7 : p7;
+      }
+    }
+    s_nb = nb;
   }
   __syncthreads();
   const unsigned long long nb = s_nb;
