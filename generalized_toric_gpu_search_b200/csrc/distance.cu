@@ -50,86 +50,6 @@ __constant__ uint8_t c_inv[8];
 __constant__ unsigned long long c_binom[22][22];
 __constant__ unsigned long long c_pow7[22];
 
-// Tiles for the information sets of toric codes.  The 49 torus points are
-// Z_7^2 by discrete logarithm (point (x, y) = (alpha^a, alpha^b)); the torus
-// translations (a, b) -> (a + s, b + t) permute the columns and map every
-// toric code onto itself.  c_tile_mask[k] is a k-point set T (bit 7a + b)
-// with c_tile_m[k] pairwise disjoint translates T + c_tile_shift[k][i].
-constexpr int kTileMaxShifts = 8;
-__constant__ unsigned long long c_tile_mask[kMaxExactK + 1];
-__constant__ int c_tile_m[kMaxExactK + 1];
-__constant__ uint8_t c_tile_shift[kMaxExactK + 1][kTileMaxShifts][2];
-
-// Deterministic search, per k, for a tile with as many disjoint translates
-// as fit (up to min(8, 49 / k)): random translation sets and a randomized
-// greedy independent set in the Cayley graph of their differences.
-struct TileTable {
-  unsigned long long mask[kMaxExactK + 1];
-  int m[kMaxExactK + 1];
-  uint8_t shift[kMaxExactK + 1][kTileMaxShifts][2];
-};
-
-static TileTable search_tiles() {
-  TileTable tt{};
-  uint64_t s = 0x243F6A8885A308D3ull;
-  auto next = [&s]() {
-    s = splitmix64(s);
-    return s;
-  };
-  for (int k = 1; k <= kMaxExactK; ++k) {
-    tt.m[k] = 0;
-    for (int m = std::min(kTileMaxShifts, kN / k); m >= 1 && tt.m[k] == 0; --m) {
-      for (int trial = 0; trial < 400 && tt.m[k] == 0; ++trial) {
-        int sh[kTileMaxShifts][2] = {{0, 0}};
-        bool distinct = true;
-        for (int i = 1; i < m; ++i) {
-          sh[i][0] = int(next() % 7ull);
-          sh[i][1] = int(next() % 7ull);
-          for (int j = 0; j < i; ++j)
-            if (sh[j][0] == sh[i][0] && sh[j][1] == sh[i][1]) distinct = false;
-        }
-        if (!distinct) continue;
-        // differences t_i - t_j (i != j)
-        int diff[kTileMaxShifts * kTileMaxShifts][2];
-        int nd = 0;
-        for (int i = 0; i < m; ++i)
-          for (int j = 0; j < m; ++j)
-            if (i != j) {
-              diff[nd][0] = (sh[i][0] - sh[j][0] + 7) % 7;
-              diff[nd][1] = (sh[i][1] - sh[j][1] + 7) % 7;
-              ++nd;
-            }
-        for (int attempt = 0; attempt < 24 && tt.m[k] == 0; ++attempt) {
-          int order[kN];
-          for (int i = 0; i < kN; ++i) order[i] = i;
-          for (int i = kN - 1; i > 0; --i) std::swap(order[i], order[int(next() % uint64_t(i + 1))]);
-          unsigned long long taken = 0ull, banned = 0ull;
-          int size = 0;
-          for (int oi = 0; oi < kN && size < k; ++oi) {
-            const int p = order[oi];
-            if ((banned >> p) & 1ull) continue;
-            taken |= 1ull << p;
-            banned |= 1ull << p;
-            ++size;
-            const int a = p / 7, b = p % 7;
-            for (int d = 0; d < nd; ++d)
-              banned |= 1ull << (((a + diff[d][0]) % 7) * 7 + (b + diff[d][1]) % 7);
-          }
-          if (size == k) {
-            tt.mask[k] = taken;
-            tt.m[k] = m;
-            for (int i = 0; i < m; ++i) {
-              tt.shift[k][i][0] = uint8_t(sh[i][0]);
-              tt.shift[k][i][1] = uint8_t(sh[i][1]);
-            }
-          }
-        }
-      }
-    }
-  }
-  return tt;
-}
-
 static bool g_tables_ready[64] = {false};
 
 int upload_field_tables(int device) {
@@ -156,11 +76,6 @@ int upload_field_tables(int device) {
   e = cudaMemcpyToSymbol(c_binom, binom, sizeof(binom));
   if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_pow7, pow7, sizeof(pow7));
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyToSymbol(c_binom)");
-  static const TileTable tiles = search_tiles();
-  e = cudaMemcpyToSymbol(c_tile_mask, tiles.mask, sizeof(tiles.mask));
-  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_tile_m, tiles.m, sizeof(tiles.m));
-  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_tile_shift, tiles.shift, sizeof(tiles.shift));
-  if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyToSymbol(c_tile)");
   g_tables_ready[device] = true;
   return TG_OK;
 }

@@ -43,6 +43,7 @@ struct CodeDesc {
 
 constexpr int32_t kDecidedFlag = 1;  // value known after preparation
 constexpr int32_t kIsCodeFlag = 2;   // evaluated by information sets
+constexpr int32_t kTorusBoundFlag = 4;  // one set, bound ceil(49 (L + 1) / k) (toric M)
 
 constexpr int kIsMaxSets = 8;     // information sets per code
 constexpr int kIsMaxRows = 64;    // sets x k per code

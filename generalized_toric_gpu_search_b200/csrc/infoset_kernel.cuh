@@ -168,60 +168,6 @@ __device__ __forceinline__ void is_reorder_columns(uint64_t piv, uint64_t& p0, u
   p2 = q2;
 }
 
-// Discrete logarithms of the field elements 1..7 (alpha = x; index 0 unused)
-// and inverses modulo 7.
-__constant__ uint8_t c_alpha_log[8] = {0, 0, 1, 3, 2, 6, 4, 5};
-__constant__ uint8_t c_inv7[7] = {0, 1, 4, 5, 2, 3, 6};
-
-// The columns of try t's random affine image E1 = A T + s of the k-point
-// tile (e1), and of its translates A (T + t_i) + s = E1 + A t_i (cover).
-// Column j is the torus point (1 + j / 7, 1 + j % 7), i.e. (alpha^a, alpha^b)
-// with (a, b) its logarithms.  A is invertible, so the translates stay
-// pairwise disjoint, and E1 + A t_i is a torus translate of E1.
-__device__ void is_tile_image(int lane, int k, int m_t, int t, uint64_t& e1, uint64_t& cover) {
-  uint64_t sd = splitmix64(0xC6A4A7935BD1E995ull + uint64_t(t) * 0x9E3779B97F4A7C15ull);
-  int p, q, r, s, det;
-  do {
-    p = int(sd % 7ull);
-    sd = splitmix64(sd);
-    q = int(sd % 7ull);
-    sd = splitmix64(sd);
-    r = int(sd % 7ull);
-    sd = splitmix64(sd);
-    s = int(sd % 7ull);
-    sd = splitmix64(sd);
-    det = ((p * s - q * r) % 7 + 7) % 7;
-  } while (det == 0);
-  const int u = int(sd % 7ull);
-  sd = splitmix64(sd);
-  const int v = int(sd % 7ull);
-  const int di = c_inv7[det];  // A^-1 = det^-1 (s, -q; -r, p)
-  const int i00 = (s * di) % 7, i01 = ((7 - q) * di) % 7;
-  const int i10 = ((7 - r) * di) % 7, i11 = (p * di) % 7;
-  const uint64_t tile = c_tile_mask[k];
-  bool in_e1[2] = {false, false}, in_cov[2] = {false, false};
-#pragma unroll
-  for (int half = 0; half < 2; ++half) {
-    const int col = lane + 32 * half;
-    if (col >= kN) continue;
-    const int da = (c_alpha_log[1 + col / 7] - u + 7) % 7;
-    const int db = (c_alpha_log[1 + col % 7] - v + 7) % 7;
-    const int za = (i00 * da + i01 * db) % 7, zb = (i10 * da + i11 * db) % 7;
-    for (int i = 0; i < m_t; ++i) {
-      const int ta = (za - c_tile_shift[k][i][0] + 7) % 7;
-      const int tb = (zb - c_tile_shift[k][i][1] + 7) % 7;
-      if ((tile >> (ta * 7 + tb)) & 1ull) {
-        in_cov[half] = true;
-        if (i == 0) in_e1[half] = true;
-      }
-    }
-  }
-  e1 = uint64_t(__ballot_sync(0xffffffffu, in_e1[0])) |
-       (uint64_t(__ballot_sync(0xffffffffu, in_e1[1])) << 32);
-  cover = uint64_t(__ballot_sync(0xffffffffu, in_cov[0])) |
-          (uint64_t(__ballot_sync(0xffffffffu, in_cov[1])) << 32);
-}
-
 // Writes the rows of one set: g and the six Gray-step deltas per row.
 __device__ __forceinline__ void is_store_set(V6* dst, int lane, int k, uint64_t p0, uint64_t p1,
                                              uint64_t p2) {
@@ -262,116 +208,78 @@ __global__ void __launch_bounds__(kIsPrepWarps * 32) prep_infoset_kernel(DistArg
       o2 |= ((v >> 2) & 1ull) << j;
     }
   }
-  const int cap_sets = min(kIsMaxSets, kIsMaxRows / k);
-  const int full_max = min(cap_sets, kN / k);
-  const bool partial_ok = full_max < cap_sets && kN - full_max * k > 0;
-  const int ideal = full_max * 64 + (partial_ok ? min(k, kN - full_max * k) : 0);
-  int best_score = -1, best_t = 0;
+  V6* base = a.is_rows + size_t(c) * a.is_stride;
   bool deficient = false;
-  for (int t = 0; t < kIsTries; ++t) {
-    is_make_order(s_ord[wl], t, lane);
-    uint64_t p0 = o0, p1 = o1, p2 = o2, used = 0ull;
-    int m = 0, rp = 0;
-    while (m < full_max) {
-      const int r = is_gauss_jordan(lane, k, p0, p1, p2, used, s_ord[wl]);
-      if (r < k) {
-        rp = r;
-        break;
-      }
-      ++m;
-    }
-    if (t == 0 && m == 0) {
-      deficient = true;  // dependent rows: some nonzero message gives the zero codeword
-      break;
-    }
-    if (m == full_max && partial_ok) rp = is_gauss_jordan(lane, k, p0, p1, p2, used, s_ord[wl]);
-    const int score = m * 64 + rp;
-    if (score > best_score) {
-      best_score = score;
-      best_t = t;
-    }
-    if (best_score >= ideal) break;
-  }
-  // Plan "translates" (toric M): one information set E1 whose torus
-  // translates are disjoint covers as many sets as it has translates, all
-  // enumerated by E1 alone (a translate's codewords are shifted codewords of
-  // E1's, with the same weights); a second set E2 on the leftover columns
-  // adds one more when it has full rank (or a partial one).  It replaces the
-  // plan above when its bound is at least as large at every level and it
-  // enumerates no more sets.
-  const int m_b = best_score >= 0 ? best_score / 64 : 0;
-  const int r_b = best_score >= 0 ? best_score % 64 : 0;
-  const int delta_b = (r_b > 0 && k - r_b <= kIsMaxDelta && m_b < cap_sets) ? k - r_b : 0;
-  bool use_t = false;
-  uint64_t t_e1 = 0ull, t_left = 0ull;
-  int t_full = 0, t_delta = 0;
-  bool t_e2 = false;
-  if (a.is_toric && !deficient && c_tile_m[k] >= 1) {
-    is_make_order(s_ord[wl], 0, lane);  // identity order; `used` masks select the columns
-    const int m_t = c_tile_m[k];
-    for (int t = 0; t < kIsTries && t_e1 == 0ull; ++t) {
-      uint64_t e1 = 0ull, cover = 0ull;
-      is_tile_image(lane, k, m_t, t, e1, cover);
-      uint64_t p0 = o0, p1 = o1, p2 = o2, used = ~e1 & kMask49;
-      if (is_gauss_jordan(lane, k, p0, p1, p2, used, s_ord[wl]) == k) {
-        t_e1 = e1;
-        t_left = ~cover & kMask49;
-      }
-    }
-    if (t_e1 != 0ull) {
-      uint64_t p0 = o0, p1 = o1, p2 = o2, used = ~t_left & kMask49;
-      const int r2 = t_left ? is_gauss_jordan(lane, k, p0, p1, p2, used, s_ord[wl]) : 0;
-      t_full = m_t + (r2 == k ? 1 : 0);
-      t_delta = (r2 > 0 && r2 < k && k - r2 <= kIsMaxDelta) ? k - r2 : 0;
-      t_e2 = r2 == k || t_delta > 0;
-      const int cost_t = 1 + (t_e2 ? 1 : 0);
-      const int cost_b = m_b + (delta_b > 0 ? 1 : 0);
-      bool dominates = cost_t <= cost_b;
-      for (int L = 0; L <= k && dominates; ++L) {
-        const int f_t = t_full * (L + 1) + (t_delta > 0 ? max(0, L + 1 - t_delta) : 0);
-        const int f_b = m_b * (L + 1) + (delta_b > 0 ? max(0, L + 1 - delta_b) : 0);
-        dominates = f_t >= f_b;
-      }
-      use_t = dominates;
-    }
-  }
   int n_sets = 0, m_full = 0, delta = 0;
-  if (use_t) {
-    V6* base = a.is_rows + size_t(c) * a.is_stride;
-    uint64_t p0 = o0, p1 = o1, p2 = o2, used = ~t_e1 & kMask49;
-    is_gauss_jordan(lane, k, p0, p1, p2, used, s_ord[wl]);
-    is_reorder_columns(t_e1, p0, p1, p2);
-    is_store_set(base, lane, k, p0, p1, p2);
-    n_sets = 1;
-    if (t_e2) {
-      p0 = o0;
-      p1 = o1;
-      p2 = o2;
-      used = ~t_left & kMask49;
-      is_gauss_jordan(lane, k, p0, p1, p2, used, s_ord[wl]);
-      is_reorder_columns(used & t_left, p0, p1, p2);
-      is_store_set(base + size_t(k) * kIsVecPerRow, lane, k, p0, p1, p2);
-      n_sets = 2;
-    }
-    m_full = t_full;
-    delta = t_delta;
-  } else if (!deficient) {
-    is_make_order(s_ord[wl], best_t, lane);
+  int32_t flags = kIsCodeFlag;
+  if (a.is_toric) {
+    // One information set, the first k independent columns: the torus
+    // translations act regularly on the columns and map the code onto
+    // itself, so E's 49 translates are information sets whose light
+    // codewords are shifted copies of E's (with the same weights).  After
+    // levels 1..L on E alone, a codeword not seen has weight >= L + 1 on every
+    // translate, and each column lies in k of them: k wt >= 49 (L + 1).
+    is_make_order(s_ord[wl], 0, lane);
     uint64_t p0 = o0, p1 = o1, p2 = o2, used = 0ull;
-    V6* base = a.is_rows + size_t(c) * a.is_stride;
-    while (n_sets < cap_sets) {
-      const uint64_t used_before = used;
-      const int r = is_gauss_jordan(lane, k, p0, p1, p2, used, s_ord[wl]);
-      if (r < k && (r == 0 || k - r > kIsMaxDelta)) break;
-      uint64_t q0 = p0, q1 = p1, q2 = p2;
-      is_reorder_columns(used & ~used_before, q0, q1, q2);
-      is_store_set(base + size_t(n_sets) * k * kIsVecPerRow, lane, k, q0, q1, q2);
-      ++n_sets;
-      if (r < k) {
-        delta = k - r;
+    if (is_gauss_jordan(lane, k, p0, p1, p2, used, s_ord[wl]) < k) {
+      deficient = true;  // dependent rows: some nonzero message gives the zero codeword
+    } else {
+      is_reorder_columns(used, p0, p1, p2);
+      is_store_set(base, lane, k, p0, p1, p2);
+      n_sets = 1;
+      m_full = 1;
+      flags |= kTorusBoundFlag;
+    }
+  } else {
+    // Disjoint information sets, greedily along a column order: the identity
+    // and up to kIsTries - 1 shuffles, keeping the most full sets and then the
+    // largest partial rank.
+    const int cap_sets = min(kIsMaxSets, kIsMaxRows / k);
+    const int full_max = min(cap_sets, kN / k);
+    const bool partial_ok = full_max < cap_sets && kN - full_max * k > 0;
+    const int ideal = full_max * 64 + (partial_ok ? min(k, kN - full_max * k) : 0);
+    int best_score = -1, best_t = 0;
+    for (int t = 0; t < kIsTries; ++t) {
+      is_make_order(s_ord[wl], t, lane);
+      uint64_t p0 = o0, p1 = o1, p2 = o2, used = 0ull;
+      int m = 0, rp = 0;
+      while (m < full_max) {
+        const int r = is_gauss_jordan(lane, k, p0, p1, p2, used, s_ord[wl]);
+        if (r < k) {
+          rp = r;
+          break;
+        }
+        ++m;
+      }
+      if (t == 0 && m == 0) {
+        deficient = true;  // dependent rows: some nonzero message gives the zero codeword
         break;
       }
-      ++m_full;
+      if (m == full_max && partial_ok) rp = is_gauss_jordan(lane, k, p0, p1, p2, used, s_ord[wl]);
+      const int score = m * 64 + rp;
+      if (score > best_score) {
+        best_score = score;
+        best_t = t;
+      }
+      if (best_score >= ideal) break;
+    }
+    if (!deficient) {
+      is_make_order(s_ord[wl], best_t, lane);
+      uint64_t p0 = o0, p1 = o1, p2 = o2, used = 0ull;
+      while (n_sets < cap_sets) {
+        const uint64_t used_before = used;
+        const int r = is_gauss_jordan(lane, k, p0, p1, p2, used, s_ord[wl]);
+        if (r < k && (r == 0 || k - r > kIsMaxDelta)) break;
+        uint64_t q0 = p0, q1 = p1, q2 = p2;
+        is_reorder_columns(used & ~used_before, q0, q1, q2);
+        is_store_set(base + size_t(n_sets) * k * kIsVecPerRow, lane, k, q0, q1, q2);
+        ++n_sets;
+        if (r < k) {
+          delta = k - r;
+          break;
+        }
+        ++m_full;
+      }
     }
   }
   if (lane == 0) {
@@ -381,7 +289,7 @@ __global__ void __launch_bounds__(kIsPrepWarps * 32) prep_infoset_kernel(DistArg
     d.H = n_sets;
     d.n_pat = delta;
     d.tmax = kN - (a.target ? a.target[c] : a.td_default);
-    d.flags = kIsCodeFlag | (deficient ? kDecidedFlag : 0);
+    d.flags = flags | (deficient ? kDecidedFlag : 0);
     d.set_id = c;
     d.n_tasks = 0ull;
     a.desc[c] = d;
@@ -418,7 +326,9 @@ __global__ void plan_level_kernel(DistArgs a, int w) {
   if ((d.flags & kIsCodeFlag) != 0 && (d.flags & kDecidedFlag) == 0 && a.abort[c] == 0) {
     const int best = a.is_best[c];
     const int L = w - 1;
-    const int bound = d.R * (L + 1) + (d.n_pat > 0 ? max(0, L + 1 - d.n_pat) : 0);
+    const int bound = (d.flags & kTorusBoundFlag)
+                          ? (kN * (L + 1) + d.k - 1) / d.k
+                          : d.R * (L + 1) + (d.n_pat > 0 ? max(0, L + 1 - d.n_pat) : 0);
     if (w > d.k || best <= bound || best < kN - d.tmax) {
       a.abort[c] = 1;  // exact (bound met or every message seen), or a witness
     } else {
