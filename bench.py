@@ -61,6 +61,8 @@ def launches_per_step(k_max: int, enumeration: str) -> int:
     finalize_infoset."""
     infoset = enumeration == "infoset" or (enumeration == "auto" and k_max >= 10)
     return 3 + ((2 + 3 * k_max) if infoset else 0)
+
+
 L2_FLUSH_BYTES = 256 << 20
 
 
@@ -150,6 +152,78 @@ class Dist:
 # ---------------------------------------------------------------------------
 # clocks during the timed region
 # ---------------------------------------------------------------------------
+
+class NvmlClockSampler:
+    """Samples SM clock, power and clock-event reasons every `period` seconds
+    from a thread through NVML (read-only queries)."""
+
+    REASONS = {"hw_slowdown": "nvmlClocksEventReasonHwSlowdown",
+               "hw_thermal_slowdown": "nvmlClocksEventReasonHwThermalSlowdown",
+               "sw_thermal_slowdown": "nvmlClocksEventReasonSwThermalSlowdown",
+               "sw_power_cap": "nvmlClocksEventReasonSwPowerCap"}
+
+    def __init__(self, cuda_index: int, period: float = 0.005):
+        import threading
+
+        import pynvml
+        import torch
+
+        self.nv = pynvml
+        pynvml.nvmlInit()
+        handle = None
+        try:
+            uuid = str(torch.cuda.get_device_properties(cuda_index).uuid)
+            handle = pynvml.nvmlDeviceGetHandleByUUID(
+                uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:  # noqa: BLE001 - fall back to the index
+            handle = pynvml.nvmlDeviceGetHandleByIndex(cuda_index)
+        self.h = handle
+        self.period = period
+        self.rows: list[tuple] = []
+        self._stop = threading.Event()
+        self._thread = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self) -> None:
+        nv = self.nv
+        while not self._stop.is_set():
+            try:
+                self.rows.append((nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM),
+                                  nv.nvmlDeviceGetPowerUsage(self.h) / 1000.0,
+                                  nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)))
+            except Exception:  # noqa: BLE001 - a failed read is skipped
+                pass
+            self._stop.wait(self.period)
+
+    def start(self) -> None:
+        self._thread.start()
+
+    def stop(self) -> dict:
+        self._stop.set()
+        self._thread.join(timeout=5)
+        nv = self.nv
+        try:
+            smax = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
+        except Exception:  # noqa: BLE001
+            smax = None
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": smax, "reasons": ["no samples"]}
+        reasons = set()
+        for _, _, mask in self.rows:
+            for name, attr in self.REASONS.items():
+                if mask & getattr(nv, attr, 0):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(r[0] for r in self.rows), "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(self.rows),
+                "power_w_max": max(r[1] for r in self.rows), "source": "nvml"}
+
+
+def clock_sampler(cuda_index: int):
+    """NVML sampler when available, else nvidia-smi."""
+    try:
+        return NvmlClockSampler(cuda_index)
+    except Exception:  # noqa: BLE001 - no NVML: nvidia-smi
+        return ClockSampler(cuda_index)
+
 
 class ClockSampler:
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -520,7 +594,7 @@ def run_b200_arm(args, d: Dist) -> None:
     paths = runner.path_counters(stream)
 
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
-    clocks = ClockSampler(dev)
+    clocks = clock_sampler(dev)
     d.barrier()
     torch.cuda.synchronize()
     clocks.start()
