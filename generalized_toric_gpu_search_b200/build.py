@@ -67,6 +67,34 @@ def build(force: bool = False, ptxas_verbose: bool = False) -> Path:
     return LIB_PATH
 
 
+def pack_ext_path() -> Path:
+    import sysconfig
+
+    return PKG_DIR / ("_pack" + (sysconfig.get_config_var("EXT_SUFFIX") or ".so"))
+
+
+def build_pack(force: bool = False) -> Path:
+    """Compiles the host-side batch packer (csrc/pack.c, CPython C API) with
+    the system C compiler (skipped when up to date)."""
+    import sysconfig
+
+    out = pack_ext_path()
+    src = CSRC / "pack.c"
+    if not force and out.exists() and out.stat().st_mtime >= src.stat().st_mtime:
+        return out
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        raise RuntimeError("no C compiler found for the batch packer")
+    cmd = [cc, "-O2", "-shared", "-fPIC", "-I" + sysconfig.get_paths()["include"], str(src),
+           "-o", str(out) + ".tmp"]
+    proc = subprocess.run(cmd, capture_output=True, text=True)
+    if proc.returncode != 0:
+        raise RuntimeError("packer build failed:\n%s\n%s" % (" ".join(cmd), proc.stderr))
+    os.replace(str(out) + ".tmp", out)
+    return out
+
+
 if __name__ == "__main__":
     build(force=True, ptxas_verbose="--ptxas-verbose" in sys.argv)
+    build_pack(force=True)
     print(LIB_PATH)

@@ -84,8 +84,34 @@ class ToricContext:
             pass
 
 
+def _load_packer():
+    try:
+        from . import _pack
+    except ImportError:
+        return None
+    return _pack
+
+
+_PACKER = _load_packer()
+
+
 def pack_sets(batched_indices) -> tuple[np.ndarray, np.ndarray, int]:
-    """Flattens a list of index lists into (flat int32, offsets int64, k_max)."""
+    """Flattens a list of index lists into (flat int32, offsets int64, k_max).
+
+    Sequences of Python ints go through the C packer (csrc/pack.c); other
+    element types (floats, numpy arrays of them) through numpy.  An index
+    that does not fit int32 comes back as -1, so a 0..48 range check on the
+    flat array rejects it.
+    """
+    if _PACKER is not None:
+        try:
+            flat_b, off_b, k_max, _ = _PACKER.pack(batched_indices)
+        except (TypeError, OverflowError):
+            pass
+        else:
+            offsets = np.frombuffer(off_b, dtype=np.int64)
+            flat = np.frombuffer(flat_b, dtype=np.int32, count=int(offsets[-1]))
+            return flat, offsets, int(k_max)
     lengths = np.fromiter((len(s) for s in batched_indices), dtype=np.int64,
                           count=len(batched_indices))
     offsets = np.zeros(len(batched_indices) + 1, dtype=np.int64)

@@ -1,0 +1,76 @@
+"""Host batch packer (csrc/pack.c) against the numpy packing path.
+
+The max_zeros entry points take a list of index lists
+(kernel_cuda_bp.py:290-323); both packers must give the same int32 flat
+array, int64 offsets and k_max, including for empty and ragged batches.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from generalized_toric_gpu_search_b200 import build as lib_build
+from generalized_toric_gpu_search_b200 import distance as D
+
+
+@pytest.fixture(scope="module")
+def packer():
+    lib_build.build_pack()
+    from generalized_toric_gpu_search_b200 import _pack
+
+    return _pack
+
+
+def _numpy_pack(batch, monkeypatch):
+    with monkeypatch.context() as m:
+        m.setattr(D, "_PACKER", None)
+        return D.pack_sets(batch)
+
+
+def _same(a, b):
+    assert a[0].dtype == b[0].dtype == np.int32
+    assert a[1].dtype == b[1].dtype == np.int64
+    np.testing.assert_array_equal(a[0], b[0])
+    np.testing.assert_array_equal(a[1], b[1])
+    assert a[2] == b[2]
+
+
+@pytest.mark.parametrize("batch", [
+    [], [[]], [[], []], [[0]], [[48, 0, 17]], [[1, 2], [], [3, 4, 5, 6]],
+    [tuple(range(21))], [list(range(49))],
+])
+def test_edge_batches(packer, monkeypatch, batch):
+    monkeypatch.setattr(D, "_PACKER", packer)
+    _same(D.pack_sets(batch), _numpy_pack(batch, monkeypatch))
+
+
+def test_random_ragged(packer, monkeypatch):
+    rng = np.random.default_rng(7)
+    batch = [rng.choice(49, size=int(rng.integers(0, 22)), replace=False).tolist()
+             for _ in range(3000)]
+    monkeypatch.setattr(D, "_PACKER", packer)
+    got = D.pack_sets(batch)
+    _same(got, _numpy_pack(batch, monkeypatch))
+    assert got[0].flags.writeable and got[1].flags.writeable
+
+
+def test_out_of_range_flags(packer):
+    flat, off, k_max, bad = packer.pack([[1, 2], [49]])
+    assert bad and k_max == 2
+    assert np.frombuffer(flat, np.int32).tolist() == [1, 2, 49]
+    _, _, _, bad = packer.pack([[0, 48]])
+    assert not bad
+    # values beyond int32 come back as -1 so a range check rejects them
+    flat, _, _, bad = packer.pack([[2**40, 3]])
+    assert bad and np.frombuffer(flat, np.int32).tolist() == [-1, 3]
+
+
+def test_other_element_types_fall_back(packer, monkeypatch):
+    monkeypatch.setattr(D, "_PACKER", packer)
+    with pytest.raises(TypeError):
+        packer.pack([[1.0, 2]])
+    flat, off, k = D.pack_sets([[1.0, 2], np.array([3, 4, 5])])
+    assert flat.tolist() == [1, 2, 3, 4, 5] and off.tolist() == [0, 2, 5] and k == 3
+    with pytest.raises(TypeError):
+        packer.pack(5)
