@@ -121,6 +121,25 @@ __device__ __forceinline__ int last_le(const uint64_t* a, int n, uint64_t x) {
   return lo;
 }
 
+// The same search starting from a known lo (a[lo] <= x), galloping forward:
+// O(log distance) loads when x lies close after a[lo].
+template <bool kCG = false>
+__device__ __forceinline__ int last_le_from(const uint64_t* a, int lo, int n, uint64_t x) {
+  int hi = n - 1;
+  for (int step = 1; lo + step < n; step <<= 1) {
+    if (ld_u64<kCG>(a + lo + step) > x) {
+      hi = lo + step - 1;
+      break;
+    }
+    lo += step;
+  }
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (ld_u64<kCG>(a + mid) <= x) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
 // splitmix64 finaliser (kernel_cuda_bp.py:47-52, kernel.py:10-15).
 __host__ __device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
   x += 0x9E3779B97F4A7C15ull;

@@ -530,26 +530,52 @@ __device__ __forceinline__ void pl3_xor(Pl3& a, const Pl3& b) {
   a.x2 ^= b.x2;
 }
 
-// The rare path of a block: rebuilds P (the support's rows other than digit
-// 0, at each digit-1 value and the block-b values of digits 2..) and counts
-// the block's 49 codewords exactly.
-template <int kStride>
-__device__ __noinline__ int is_block_exact(const V6* rows, uint32_t r0, uint32_t r1, uint32_t rc,
-                                           const uint16_t* dig, int n_dig, unsigned long long b,
-                                           int wmin) {
-  V6 P = v6_ldg(rows + rc);
-  unsigned long long rest = b;
-  for (int i = 0; i < n_dig; ++i) {
-    V6 y = v6_ldg(rows + dig[i * kStride]);
-    v6_alpha_pow(y, is_block_digit(rest));
-    v6_xor(P, y);
+// c x for a constant c of GF(8), on three bit planes (x0, x1, x2) of 32
+// columns; folds to a few XORs when c is known at compile time.
+__device__ __forceinline__ void gf8_scale32(uint32_t c, uint32_t& x0, uint32_t& x1, uint32_t& x2) {
+  uint32_t r0 = 0u, r1 = 0u, r2 = 0u;
+  uint32_t a0 = x0, a1 = x1, a2 = x2;
+#pragma unroll
+  for (int b = 0; b < 3; ++b) {
+    if ((c >> b) & 1u) {
+      r0 ^= a0;
+      r1 ^= a1;
+      r2 ^= a2;
+    }
+    const uint32_t t = a2;  // a <- alpha a
+    a2 = a1;
+    a1 = a0 ^ t;
+    a0 = t;
   }
-  V6 x = v6_ldg(rows + r1);  // digit 1 through alpha^0..alpha^6
-  for (int v1 = 0; v1 < 7; ++v1) {
-    V6 Q = P;
-    v6_xor(Q, x);
-    wmin = is_sweep_exact(Q, rows + r0, wmin);
-    v6_alpha_pow(x, 1);
+  x0 = r0;
+  x1 = r1;
+  x2 = r2;
+}
+
+// The rare path of a sweep whose lower bound reaches below wmin: exact
+// weights of its seven codewords P + alpha^v g.  The low half comes from the
+// sweep's zero counts z[v] (plus zz, the zeros on g's zero columns); the high
+// half is rebuilt from Ph, P's high word without digit 1's term, plus kC r1
+// (kC = digit 1's coefficient in this sweep).
+template <uint32_t kC>
+__device__ __forceinline__ int is_sweep_fix(const int (&z)[7], int zz, uint32_t ph0,
+                                            uint32_t ph1, uint32_t ph2, const V6* g_row,
+                                            const V6* r1_row, int wmin) {
+  uint32_t d0 = __ldg(&r1_row->h0), d1 = __ldg(&r1_row->h1), d2 = __ldg(&r1_row->h2);
+  gf8_scale32(kC, d0, d1, d2);
+  ph0 ^= d0;
+  ph1 ^= d1;
+  ph2 ^= d2;
+  uint32_t g0 = __ldg(&g_row->h0), g1 = __ldg(&g_row->h1), g2 = __ldg(&g_row->h2);
+  const int lo_base = 32 - zz;
+#pragma unroll
+  for (int v = 0; v < 7; ++v) {
+    const int hi = __popc(lop3<0xFE>(ph0 ^ g0, ph1 ^ g1, ph2 ^ g2));
+    wmin = min(wmin, lo_base - z[v] + hi);
+    const uint32_t t = g2;  // g <- alpha g
+    g2 = g1;
+    g1 = g0 ^ t;
+    g0 = t;
   }
   return wmin;
 }
@@ -558,20 +584,27 @@ __device__ __noinline__ int is_block_exact(const V6* rows, uint32_t r0, uint32_t
 // (column-wise; g the digit-0 row): P + alpha^v g vanishes at column j
 // exactly when W_j = alpha^v (g_j != 0) or P_j = 0 (g_j = 0).  So the zeros
 // of all seven codewords are seven one-LOP3 selections plus the zero columns
-// of g (tracked as Pz = P & gz).  bm keeps the most low-half zeros of the
-// block.
-#define TG_IS_SWEEP                                                                              \
+// of g (tracked as Pz = P & gz).  The high columns weigh at least hb, so only
+// a sweep with more than thr = 32 + hb - wmin low zeros can hold a codeword
+// lighter than wmin; that sweep is counted exactly (kC: digit 1's
+// coefficient in this sweep).
+#define TG_IS_SWEEP(kC)                                                                          \
   {                                                                                              \
-    const int z0_ = __popc(lop3<sel_lut(1)>(W.x0, W.x1, W.x2));                                  \
-    const int z1_ = __popc(lop3<sel_lut(2)>(W.x0, W.x1, W.x2));                                  \
-    const int z2_ = __popc(lop3<sel_lut(4)>(W.x0, W.x1, W.x2));                                  \
-    const int z3_ = __popc(lop3<sel_lut(3)>(W.x0, W.x1, W.x2));                                  \
-    const int z4_ = __popc(lop3<sel_lut(6)>(W.x0, W.x1, W.x2));                                  \
-    const int z5_ = __popc(lop3<sel_lut(7)>(W.x0, W.x1, W.x2));                                  \
-    const int z6_ = __popc(lop3<sel_lut(5)>(W.x0, W.x1, W.x2));                                  \
+    int z_[7];                                                                                   \
+    z_[0] = __popc(lop3<sel_lut(1)>(W.x0, W.x1, W.x2));                                          \
+    z_[1] = __popc(lop3<sel_lut(2)>(W.x0, W.x1, W.x2));                                          \
+    z_[2] = __popc(lop3<sel_lut(4)>(W.x0, W.x1, W.x2));                                          \
+    z_[3] = __popc(lop3<sel_lut(3)>(W.x0, W.x1, W.x2));                                          \
+    z_[4] = __popc(lop3<sel_lut(6)>(W.x0, W.x1, W.x2));                                          \
+    z_[5] = __popc(lop3<sel_lut(7)>(W.x0, W.x1, W.x2));                                          \
+    z_[6] = __popc(lop3<sel_lut(5)>(W.x0, W.x1, W.x2));                                          \
     const int zz_ = ngz - __popc(lop3<0xFE>(Pz.x0, Pz.x1, Pz.x2));                              \
-    bm = __vimax3_s32(bm, __vimax3_s32(z0_, z1_, z2_) + zz_,                                     \
-                      __vimax3_s32(z3_, z4_, max(z5_, z6_)) + zz_);                      \
+    const int zm_ = __vimax3_s32(__vimax3_s32(z_[0], z_[1], z_[2]),                              \
+                                 __vimax3_s32(z_[3], z_[4], z_[5]), z_[6]) + zz_;                \
+    if (__builtin_expect(zm_ > thr, 0)) {                                                        \
+      wmin = is_sweep_fix<kC>(z_, zz_, ph0, ph1, ph2, rows + r0, rows + r1, wmin);               \
+      thr = thr_base - wmin;                                                                     \
+    }                                                                                            \
   }
 #define TG_IS_MOVE(I)                                                        \
   {                                                                          \
@@ -589,12 +622,14 @@ __device__ __noinline__ int is_block_exact(const V6* rows, uint32_t r0, uint32_t
 // straight-line code.  Digit 1's six moves, in the W domain and on g's zero
 // columns, are kept in this thread's shared-memory slots ez (stride kStride);
 // the move between blocks (digits 2.., rows dig[]) is loaded a block ahead.
-// Returns the codewords evaluated.
+// P's high word without digit 1's term (which the block moves do not touch)
+// is kept for the exact count of a rare sweep.  Returns the codewords
+// evaluated.
 template <int kStride>
 __device__ __forceinline__ unsigned long long is_walk_blocks(
-    const V6& P, const V6* rows, uint32_t r0, uint32_t r1, uint32_t rc, const uint16_t* dig,
-    uint32_t* ez, int n_dig, unsigned long long b0, unsigned long long nblk, int hb, int wthr,
-    const int32_t* stop, int& wmin) {
+    const V6& P, const V6* rows, uint32_t r0, uint32_t r1, const uint16_t* dig, uint32_t* ez,
+    unsigned long long b0, unsigned long long nblk, int hb, int wthr, const int32_t* stop,
+    int& wmin) {
   const Pl3 g = pl3_lo(v6_ldg(rows + r0));
   const Pl3 h = pl3_inv(g);
   const uint32_t gz = ~(g.x0 | g.x1 | g.x2);  // low columns where g is 0
@@ -612,6 +647,17 @@ __device__ __forceinline__ unsigned long long is_walk_blocks(
   }
   Pl3 W = pl3_mul(pl3_lo(P), h);
   Pl3 Pz = pl3_and(pl3_lo(P), gz);
+  uint32_t ph0 = P.h0, ph1 = P.h1, ph2 = P.h2;
+  {
+    // digit 1 starts at alpha^0 (b0 even) or alpha^6 = 5 (b0 odd)
+    uint32_t d0 = __ldg(&rows[r1].h0), d1 = __ldg(&rows[r1].h1), d2 = __ldg(&rows[r1].h2);
+    if (b0 & 1ull) gf8_scale32(5u, d0, d1, d2);
+    ph0 ^= d0;
+    ph1 ^= d1;
+    ph2 ^= d2;
+  }
+  const int thr_base = 32 + hb;
+  int thr = thr_base - wmin;
   V6 nx;
   v6_zero(nx);
   if (nblk > 1ull) nx = v6_ldg(is_block_move<kStride>(rows, dig, b0 + 1ull));
@@ -622,25 +668,27 @@ __device__ __forceinline__ unsigned long long is_walk_blocks(
       const Pl3 d = pl3_lo(nx);
       pl3_xor(W, pl3_mul(d, h));
       pl3_xor(Pz, pl3_and(d, gz));
+      ph0 ^= nx.h0;
+      ph1 ^= nx.h1;
+      ph2 ^= nx.h2;
       if (i + 1ull < nblk) nx = v6_ldg(is_block_move<kStride>(rows, dig, b + 1ull));
     }
-    // digit 1 runs up through block b when b is even
-    int bm = 0;
+    // Digit 1 runs up from alpha^0 through block b when b is even (sweep s at
+    // alpha^s), else down from alpha^6 (sweep s at alpha^(6-s)); alpha^0..6 =
+    // 1, 2, 4, 3, 6, 7, 5.
     if ((b & 1ull) == 0ull) {
-      TG_IS_SWEEP; TG_IS_MOVE(0); TG_IS_SWEEP; TG_IS_MOVE(1); TG_IS_SWEEP; TG_IS_MOVE(2);
-      TG_IS_SWEEP; TG_IS_MOVE(3); TG_IS_SWEEP; TG_IS_MOVE(4); TG_IS_SWEEP; TG_IS_MOVE(5);
-      TG_IS_SWEEP;
+      TG_IS_SWEEP(1u); TG_IS_MOVE(0); TG_IS_SWEEP(2u); TG_IS_MOVE(1); TG_IS_SWEEP(4u);
+      TG_IS_MOVE(2); TG_IS_SWEEP(3u); TG_IS_MOVE(3); TG_IS_SWEEP(6u); TG_IS_MOVE(4);
+      TG_IS_SWEEP(7u); TG_IS_MOVE(5); TG_IS_SWEEP(5u);
     } else {
-      TG_IS_SWEEP; TG_IS_MOVE(5); TG_IS_SWEEP; TG_IS_MOVE(4); TG_IS_SWEEP; TG_IS_MOVE(3);
-      TG_IS_SWEEP; TG_IS_MOVE(2); TG_IS_SWEEP; TG_IS_MOVE(1); TG_IS_SWEEP; TG_IS_MOVE(0);
-      TG_IS_SWEEP;
+      TG_IS_SWEEP(5u); TG_IS_MOVE(5); TG_IS_SWEEP(7u); TG_IS_MOVE(4); TG_IS_SWEEP(6u);
+      TG_IS_MOVE(3); TG_IS_SWEEP(3u); TG_IS_MOVE(2); TG_IS_SWEEP(4u); TG_IS_MOVE(1);
+      TG_IS_SWEEP(2u); TG_IS_MOVE(0); TG_IS_SWEEP(1u);
     }
-    // The high columns hold the set's pivot columns, where a codeword equals
-    // its message, so they weigh at least hb: only a block whose lightest low
-    // half plus hb is below wmin can lower it, and is counted exactly.
-    if (32 - bm + hb < wmin) wmin = is_block_exact<kStride>(rows, r0, r1, rc, dig, n_dig, b, wmin);
     if (wmin < wthr) break;
-    if ((i & 15ull) == 15ull && ld_flag(stop)) break;
+    // Another task's witness (a weight below wthr) stops the code; with
+    // wthr <= 1 there is none, and the flag is not polled.
+    if (wthr > 1 && (i & 15ull) == 15ull && ld_flag(stop)) break;
   }
   return 49ull * (min(i, nblk - 1ull) + 1ull);
 }
@@ -675,13 +723,12 @@ __device__ __forceinline__ int is_walk_units(const DistArgs& a,
     const unsigned long long nblk = min(bps - b, u1 - u);
     const V6* rows = base + size_t(j) * k * kIsVecPerRow;
     // Support rows from the largest down (combinadic unranking).  The q-th
-    // row found is Gray digit q (q < w - 1); the last one (rc) has
-    // coefficient 1.  Digit 0 is swept through all seven values and stays out
+    // row found is Gray digit q (q < w - 1); the last one has coefficient 1.  Digit 0 is swept through all seven values and stays out
     // of P; digit 1 starts at alpha^0 (b even) or alpha^6 (b odd); digit
     // 2 + i starts at the Gray value of base-7 digit i of b.
     V6 P;
     v6_zero(P);
-    uint32_t r0 = 0u, r1 = 0u, rc = 0u;
+    uint32_t r0 = 0u, r1 = 0u;
     unsigned long long srank = s, rest = b;
     int rem = w, q = 0;
     for (int pos = k - 1; pos >= 0 && rem > 0; --pos) {
@@ -704,8 +751,6 @@ __device__ __forceinline__ int is_walk_units(const DistArgs& a,
             e = is_block_digit(rest);
           }
           v6_alpha_pow(g, e);
-        } else {
-          rc = R;
         }
         v6_xor(P, g);
       }
@@ -724,8 +769,7 @@ __device__ __forceinline__ int is_walk_units(const DistArgs& a,
       // that do not fit in the 17 high columns (k > 17).
       const int dj = int(j) == n_sets - 1 ? delta : 0;
       const int hb = max(0, w - dj - max(0, (k - dj) - 17));
-      ncw += is_walk_blocks<kStride>(P, rows, r0, r1, rc, dig, ez, w - 3, b, nblk, hb, wthr, stop,
-                                     wmin);
+      ncw += is_walk_blocks<kStride>(P, rows, r0, r1, dig, ez, b, nblk, hb, wthr, stop, wmin);
     }
     u += nblk;
     if (wmin < wthr) break;
@@ -749,36 +793,63 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) walk_level_kernel(DistArgs a
   unsigned long long evaluated = 0ull;
   uint16_t* my_dig = &s_dig[0][threadIdx.x];  // this thread's digit rows, stride kTPB
   uint32_t* my_ez = &s_ez[0][threadIdx.x];     // this thread's digit-1 moves, stride kTPB
+  int c0 = 0;  // code of the warp's first task; tasks are claimed in increasing order
   for (;;) {
     unsigned long long base = 0ull;
     if (lane == 0) base = atomicAdd(&a.is_hdr->counter, 32ull);
     base = __shfl_sync(0xffffffffu, base, 0);
     if (base >= total) break;
-    int c0 = 0;
-    if (lane == 0) c0 = last_le(a.is_off, a.n + 1, base);
+    if (lane == 0) c0 = last_le_from(a.is_off, c0, a.n + 1, base);
     c0 = __shfl_sync(0xffffffffu, c0, 0);
-    const unsigned long long t = base + lane;
-    if (t >= total) continue;
-    const int c = t < __ldg(a.is_off + c0 + 1) ? c0 : last_le(a.is_off, a.n + 1, t);
-    const unsigned long long r_end = __ldg(a.is_off + c + 1);
-    if (ld_flag(a.abort + c)) {
-      atomicMax(&a.is_hdr->counter, r_end);
-      continue;
+    // The code's abort flag and best weight sit in a few cache lines that
+    // every lane would poll, so lane 0 reads them for the warp's first code.
+    int abort0 = 0, best0 = 0;
+    if (lane == 0) {
+      abort0 = ld_flag(a.abort + c0);
+      best0 = ld_flag(a.is_best + c0);
     }
-    const int wthr = kN - a.desc[c].tmax;
-    const unsigned long long u0 = (t - __ldg(a.is_off + c)) * nb;
-    const unsigned long long u1 = min(u0 + nb, static_cast<unsigned long long>(a.is_units[c]));
-    unsigned long long ncw = 0ull;
-    // Codewords no lighter than the code's best so far cannot change it, so
-    // the walk starts from that best.
-    const int wmin = is_walk_units<kTPB>(a, s_binom, my_dig, my_ez, c, a.desc[c].k, w, u0, u1, wthr,
-                                         ld_flag(a.is_best + c), ncw);
-    evaluated += ncw;
-    const int best = min(atomicMin(a.is_best + c, wmin), wmin);
-    if (best < wthr) {
-      // a witness below the target distance: the code is decided
-      atomicExch(a.abort + c, 1);
-      atomicMax(&a.is_hdr->counter, r_end);
+    abort0 = __shfl_sync(0xffffffffu, abort0, 0);
+    best0 = __shfl_sync(0xffffffffu, best0, 0);
+    const unsigned long long t = base + lane;
+    int c = -1, wmin = kN + 1;
+    if (t < total) {
+      c = t < __ldg(a.is_off + c0 + 1) ? c0 : last_le_from(a.is_off, c0, a.n + 1, t);
+      if (c != c0) {
+        abort0 = ld_flag(a.abort + c);
+        best0 = ld_flag(a.is_best + c);
+      }
+      if (abort0) {
+        atomicMax(&a.is_hdr->counter, __ldg(a.is_off + c + 1));
+        c = -1;
+      } else {
+        const unsigned long long u0 = (t - __ldg(a.is_off + c)) * nb;
+        const unsigned long long u1 =
+            min(u0 + nb, static_cast<unsigned long long>(a.is_units[c]));
+        unsigned long long ncw = 0ull;
+        // Codewords no lighter than the code's best so far cannot change it,
+        // so the walk starts from that best.
+        wmin = is_walk_units<kTPB>(a, s_binom, my_dig, my_ez, c, a.desc[c].k, w, u0, u1,
+                                   kN - a.desc[c].tmax, best0, ncw);
+        evaluated += ncw;
+      }
+    }
+    // One atomic per code and warp, and only when the warp's lightest
+    // codeword improves the code's best: the lanes of a warp mostly share a
+    // code, and most tasks find nothing lighter.
+    for (unsigned pend = __ballot_sync(0xffffffffu, c >= 0); pend != 0u;) {
+      const int leader = __ffs(pend) - 1;
+      const int cl = __shfl_sync(0xffffffffu, c, leader);
+      const bool mine = c == cl;
+      const int wl = __reduce_min_sync(0xffffffffu, mine ? wmin : kN + 1);
+      pend &= ~__ballot_sync(0xffffffffu, mine);
+      if (lane == leader && wl < ld_flag(a.is_best + cl)) {
+        const int best = min(atomicMin(a.is_best + cl, wl), wl);
+        if (best < kN - a.desc[cl].tmax) {
+          // a witness below the target distance: the code is decided
+          atomicExch(a.abort + cl, 1);
+          atomicMax(&a.is_hdr->counter, __ldg(a.is_off + cl + 1));
+        }
+      }
     }
   }
   for (int o = 16; o > 0; o >>= 1) evaluated += __shfl_xor_sync(0xffffffffu, evaluated, o);
