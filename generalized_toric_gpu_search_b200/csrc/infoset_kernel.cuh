@@ -602,7 +602,7 @@ __device__ __forceinline__ int is_sweep_fix(const int (&z)[7], int zz, uint32_t 
     const int zm_ = __vimax3_s32(__vimax3_s32(z_[0], z_[1], z_[2]),                              \
                                  __vimax3_s32(z_[3], z_[4], z_[5]), z_[6]) + zz_;                \
     if (__builtin_expect(zm_ > thr, 0)) {                                                        \
-      wmin = is_sweep_fix<kC>(z_, zz_, ph0, ph1, ph2, rows + r0, rows + r1, wmin);               \
+      wmin = is_sweep_fix<kC>(z_, zz_, qh0, qh1, qh2, rows + r0, rows + r1, wmin);               \
       thr = thr_base - wmin;                                                                     \
     }                                                                                            \
   }
@@ -618,12 +618,15 @@ __device__ __forceinline__ int is_sweep_fix(const int (&z)[7], int zz, uint32_t 
 
 // Walks blocks [b0, b0 + nblk) of one support; P is the sum of its rows other
 // than digit 0 at the start of block b0.  Each block is 7 sweeps of digit 0
-// (row r0) with digit 1 (row r1) moving between them: 49 codewords of
-// straight-line code.  Digit 1's six moves, in the W domain and on g's zero
-// columns, are kept in this thread's shared-memory slots ez (stride kStride);
-// the move between blocks (digits 2.., rows dig[]) is loaded a block ahead.
-// P's high word without digit 1's term (which the block moves do not touch)
-// is kept for the exact count of a rare sweep.  Returns the codewords
+// (row r0) with digit 1 (row r1) stepping alpha^0 .. alpha^6 between them:
+// 49 codewords of straight-line code, the same in every block, so the lanes
+// of a warp never split on the block's parity.  Digit 1's six steps, in the
+// W domain and on g's zero columns, are kept in this thread's shared-memory
+// slots ez (stride kStride), and its return alpha^6 -> alpha^0 in slots
+// 36..38; the move between blocks (digits 2.., rows dig[]) is loaded a block
+// ahead.
+// P's high word without digit 1's term (qh, which only the block moves
+// change) is kept for the exact count of a rare sweep.  Returns the codewords
 // evaluated.
 template <int kStride>
 __device__ __forceinline__ unsigned long long is_walk_blocks(
@@ -645,17 +648,19 @@ __device__ __forceinline__ unsigned long long is_walk_blocks(
     ez[(6 * i + 4) * kStride] = d.x1 & gz;
     ez[(6 * i + 5) * kStride] = d.x2 & gz;
   }
+  {
+    // (alpha^6 + alpha^0) r1 = alpha^2 r1
+    const Pl3 r = pl3_lo(v6_ldg(rows + r1));
+    ez[36 * kStride] = r.x1;
+    ez[37 * kStride] = r.x1 ^ r.x2;
+    ez[38 * kStride] = r.x0 ^ r.x2;
+  }
   Pl3 W = pl3_mul(pl3_lo(P), h);
   Pl3 Pz = pl3_and(pl3_lo(P), gz);
-  uint32_t ph0 = P.h0, ph1 = P.h1, ph2 = P.h2;
-  {
-    // digit 1 starts at alpha^0 (b0 even) or alpha^6 = 5 (b0 odd)
-    uint32_t d0 = __ldg(&rows[r1].h0), d1 = __ldg(&rows[r1].h1), d2 = __ldg(&rows[r1].h2);
-    if (b0 & 1ull) gf8_scale32(5u, d0, d1, d2);
-    ph0 ^= d0;
-    ph1 ^= d1;
-    ph2 ^= d2;
-  }
+  // digit 1 starts at alpha^0
+  uint32_t qh0 = P.h0 ^ __ldg(&rows[r1].h0);
+  uint32_t qh1 = P.h1 ^ __ldg(&rows[r1].h1);
+  uint32_t qh2 = P.h2 ^ __ldg(&rows[r1].h2);
   const int thr_base = 32 + hb;
   int thr = thr_base - wmin;
   V6 nx;
@@ -665,26 +670,22 @@ __device__ __forceinline__ unsigned long long is_walk_blocks(
   for (; i < nblk; ++i) {
     const unsigned long long b = b0 + i;
     if (i) {
-      const Pl3 d = pl3_lo(nx);
+      // digits 2.. move to block b, digit 1 returns to alpha^0
+      Pl3 d = pl3_lo(nx);
+      d.x0 ^= ez[36 * kStride];
+      d.x1 ^= ez[37 * kStride];
+      d.x2 ^= ez[38 * kStride];
       pl3_xor(W, pl3_mul(d, h));
       pl3_xor(Pz, pl3_and(d, gz));
-      ph0 ^= nx.h0;
-      ph1 ^= nx.h1;
-      ph2 ^= nx.h2;
+      qh0 ^= nx.h0;
+      qh1 ^= nx.h1;
+      qh2 ^= nx.h2;
       if (i + 1ull < nblk) nx = v6_ldg(is_block_move<kStride>(rows, dig, b + 1ull));
     }
-    // Digit 1 runs up from alpha^0 through block b when b is even (sweep s at
-    // alpha^s), else down from alpha^6 (sweep s at alpha^(6-s)); alpha^0..6 =
-    // 1, 2, 4, 3, 6, 7, 5.
-    if ((b & 1ull) == 0ull) {
-      TG_IS_SWEEP(1u); TG_IS_MOVE(0); TG_IS_SWEEP(2u); TG_IS_MOVE(1); TG_IS_SWEEP(4u);
-      TG_IS_MOVE(2); TG_IS_SWEEP(3u); TG_IS_MOVE(3); TG_IS_SWEEP(6u); TG_IS_MOVE(4);
-      TG_IS_SWEEP(7u); TG_IS_MOVE(5); TG_IS_SWEEP(5u);
-    } else {
-      TG_IS_SWEEP(5u); TG_IS_MOVE(5); TG_IS_SWEEP(7u); TG_IS_MOVE(4); TG_IS_SWEEP(6u);
-      TG_IS_MOVE(3); TG_IS_SWEEP(3u); TG_IS_MOVE(2); TG_IS_SWEEP(4u); TG_IS_MOVE(1);
-      TG_IS_SWEEP(2u); TG_IS_MOVE(0); TG_IS_SWEEP(1u);
-    }
+    // sweep s at digit-1 coefficient alpha^s; alpha^0..6 = 1, 2, 4, 3, 6, 7, 5
+    TG_IS_SWEEP(1u); TG_IS_MOVE(0); TG_IS_SWEEP(2u); TG_IS_MOVE(1); TG_IS_SWEEP(4u);
+    TG_IS_MOVE(2); TG_IS_SWEEP(3u); TG_IS_MOVE(3); TG_IS_SWEEP(6u); TG_IS_MOVE(4);
+    TG_IS_SWEEP(7u); TG_IS_MOVE(5); TG_IS_SWEEP(5u);
     if (wmin < wthr) break;
     // Another task's witness (a weight below wthr) stops the code; with
     // wthr <= 1 there is none, and the flag is not polled.
@@ -723,9 +724,10 @@ __device__ __forceinline__ int is_walk_units(const DistArgs& a,
     const unsigned long long nblk = min(bps - b, u1 - u);
     const V6* rows = base + size_t(j) * k * kIsVecPerRow;
     // Support rows from the largest down (combinadic unranking).  The q-th
-    // row found is Gray digit q (q < w - 1); the last one has coefficient 1.  Digit 0 is swept through all seven values and stays out
-    // of P; digit 1 starts at alpha^0 (b even) or alpha^6 (b odd); digit
-    // 2 + i starts at the Gray value of base-7 digit i of b.
+    // row found is Gray digit q (q < w - 1); the last one has coefficient 1.
+    // Digit 0 is swept through all seven values and stays out of P; digit 1
+    // starts every block at alpha^0; digit 2 + i starts at the Gray value of
+    // base-7 digit i of b.
     V6 P;
     v6_zero(P);
     uint32_t r0 = 0u, r1 = 0u;
@@ -742,15 +744,12 @@ __device__ __forceinline__ int is_walk_units(const DistArgs& a,
       } else {
         V6 g = v6_ldg(rows + R);
         if (rem > 0) {
-          int e;
           if (q == 1) {
             r1 = R;
-            e = (b & 1ull) ? 6 : 0;
           } else {
             dig[(q - 2) * kStride] = uint16_t(R);
-            e = is_block_digit(rest);
+            v6_alpha_pow(g, is_block_digit(rest));
           }
-          v6_alpha_pow(g, e);
         }
         v6_xor(P, g);
       }
@@ -783,7 +782,7 @@ template <int kTPB, int kMinBlocks>
 __global__ void __launch_bounds__(kTPB, kMinBlocks) walk_level_kernel(DistArgs a, int w) {
   __shared__ unsigned long long s_binom[kIsBinom][kIsBinom];
   __shared__ uint16_t s_dig[kIsMaxDigits][kTPB];
-  __shared__ uint32_t s_ez[36][kTPB];
+  __shared__ uint32_t s_ez[39][kTPB];
   for (int i = threadIdx.x; i < kIsBinom * kIsBinom; i += kTPB)
     s_binom[i / kIsBinom][i % kIsBinom] = c_binom[i / kIsBinom][i % kIsBinom];
   __syncthreads();
