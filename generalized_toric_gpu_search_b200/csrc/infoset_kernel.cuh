@@ -584,26 +584,46 @@ __device__ __forceinline__ int is_sweep_fix(const int (&z)[7], int zz, uint32_t 
 // (column-wise; g the digit-0 row): P + alpha^v g vanishes at column j
 // exactly when W_j = alpha^v (g_j != 0) or P_j = 0 (g_j = 0).  So the zeros
 // of all seven codewords are seven one-LOP3 selections plus the zero columns
-// of g (tracked as Pz = P & gz).  The high columns weigh at least hb, so only
-// a sweep with more than thr = 32 + hb - wmin low zeros can hold a codeword
-// lighter than wmin; that sweep is counted exactly (kC: digit 1's
-// coefficient in this sweep).
-#define TG_IS_SWEEP(kC)                                                                          \
+// of g (tracked as Pz = P & gz: ngz less its nonzero columns).  The high
+// columns weigh at least hb, so only a sweep with more than thr = 32 + hb -
+// wmin low zeros can hold a codeword lighter than wmin; that sweep is counted
+// exactly (kC: digit 1's coefficient in this sweep).  thz = thr - ngz is the
+// test on the selection count less Pz's nonzero columns.
+#define TG_IS_ZCOUNTS(z_)                                                                        \
+  int z_[7];                                                                                     \
+  z_[0] = __popc(lop3<sel_lut(1)>(W.x0, W.x1, W.x2));                                            \
+  z_[1] = __popc(lop3<sel_lut(2)>(W.x0, W.x1, W.x2));                                            \
+  z_[2] = __popc(lop3<sel_lut(4)>(W.x0, W.x1, W.x2));                                            \
+  z_[3] = __popc(lop3<sel_lut(3)>(W.x0, W.x1, W.x2));                                            \
+  z_[4] = __popc(lop3<sel_lut(6)>(W.x0, W.x1, W.x2));                                            \
+  z_[5] = __popc(lop3<sel_lut(7)>(W.x0, W.x1, W.x2));                                            \
+  z_[6] = __popc(lop3<sel_lut(5)>(W.x0, W.x1, W.x2));
+#define TG_IS_SWEEP1(kC)                                                                         \
   {                                                                                              \
-    int z_[7];                                                                                   \
-    z_[0] = __popc(lop3<sel_lut(1)>(W.x0, W.x1, W.x2));                                          \
-    z_[1] = __popc(lop3<sel_lut(2)>(W.x0, W.x1, W.x2));                                          \
-    z_[2] = __popc(lop3<sel_lut(4)>(W.x0, W.x1, W.x2));                                          \
-    z_[3] = __popc(lop3<sel_lut(3)>(W.x0, W.x1, W.x2));                                          \
-    z_[4] = __popc(lop3<sel_lut(6)>(W.x0, W.x1, W.x2));                                          \
-    z_[5] = __popc(lop3<sel_lut(7)>(W.x0, W.x1, W.x2));                                          \
-    z_[6] = __popc(lop3<sel_lut(5)>(W.x0, W.x1, W.x2));                                          \
-    const int zz_ = ngz - __popc(lop3<0xFE>(Pz.x0, Pz.x1, Pz.x2));                              \
+    TG_IS_ZCOUNTS(z_)                                                                            \
+    const int pz_ = __popc(lop3<0xFE>(Pz.x0, Pz.x1, Pz.x2));                                    \
     const int zm_ = __vimax3_s32(__vimax3_s32(z_[0], z_[1], z_[2]),                              \
-                                 __vimax3_s32(z_[3], z_[4], z_[5]), z_[6]) + zz_;                \
-    if (__builtin_expect(zm_ > thr, 0)) {                                                        \
-      wmin = is_sweep_fix<kC>(z_, zz_, qh0, qh1, qh2, rows + r0, rows + r1, wmin);               \
-      thr = thr_base - wmin;                                                                     \
+                                 __vimax3_s32(z_[3], z_[4], z_[5]), z_[6]) - pz_;                \
+    if (__builtin_expect(zm_ > thz, 0)) {                                                        \
+      wmin = is_sweep_fix<kC>(z_, ngz - pz_, qh0, qh1, qh2, rows + r0, rows + r1, wmin);         \
+      thz = thz_base - wmin;                                                                     \
+    }                                                                                            \
+  }
+// The same test on pairs of codewords: the selections of alpha^0|alpha^1,
+// alpha^2|alpha^3 and alpha^4|alpha^5 are disjoint, so each pair's count
+// bounds both of its codewords' zeros; four counts instead of seven.
+#define TG_IS_SWEEP2(kC)                                                                         \
+  {                                                                                              \
+    const int y0_ = __popc(lop3<sel_lut(1) | sel_lut(2)>(W.x0, W.x1, W.x2));                     \
+    const int y1_ = __popc(lop3<sel_lut(4) | sel_lut(3)>(W.x0, W.x1, W.x2));                     \
+    const int y2_ = __popc(lop3<sel_lut(6) | sel_lut(7)>(W.x0, W.x1, W.x2));                     \
+    const int y3_ = __popc(lop3<sel_lut(5)>(W.x0, W.x1, W.x2));                                  \
+    const int pz_ = __popc(lop3<0xFE>(Pz.x0, Pz.x1, Pz.x2));                                    \
+    const int ym_ = __vimax3_s32(y0_, y1_, max(y2_, y3_)) - pz_;                                 \
+    if (__builtin_expect(ym_ > thz, 0)) {                                                        \
+      TG_IS_ZCOUNTS(z_)                                                                          \
+      wmin = is_sweep_fix<kC>(z_, ngz - pz_, qh0, qh1, qh2, rows + r0, rows + r1, wmin);         \
+      thz = thz_base - wmin;                                                                     \
     }                                                                                            \
   }
 #define TG_IS_MOVE(I)                                                        \
@@ -615,6 +635,12 @@ __device__ __forceinline__ int is_sweep_fix(const int (&z)[7], int zz, uint32_t 
     Pz.x1 ^= ez[(6 * (I) + 4) * kStride];                                    \
     Pz.x2 ^= ez[(6 * (I) + 5) * kStride];                                    \
   }
+
+// Smallest thr at which a block is tested on pairs of codewords (with seven
+// selections of about 7/64 of the 32 low columns each, a pair's count tops 15
+// in about 0.3 % of the sweeps, against 1.3e-5 for the largest single count
+// over 14).
+constexpr int kIsPairThr = 15;
 
 // Walks blocks [b0, b0 + nblk) of one support; P is the sum of its rows other
 // than digit 0 at the start of block b0.  Each block is 7 sweeps of digit 0
@@ -661,14 +687,19 @@ __device__ __forceinline__ unsigned long long is_walk_blocks(
   uint32_t qh0 = P.h0 ^ __ldg(&rows[r1].h0);
   uint32_t qh1 = P.h1 ^ __ldg(&rows[r1].h1);
   uint32_t qh2 = P.h2 ^ __ldg(&rows[r1].h2);
-  const int thr_base = 32 + hb;
-  int thr = thr_base - wmin;
+  const int thz_base = 32 + hb - ngz;
+  int thz = thz_base - wmin;
+  // The move into block m = b0 + i + 1 changes digit 2 when m % 7 != 0 (six
+  // blocks in seven): up from alpha^(m7 - 1) when m / 7 is even, else down
+  // from alpha^(7 - m7); the rest take the general form.
+  const int n = int(nblk);  // at most 343
+  int m7 = int((b0 + 1ull) % 7ull);
+  int par = int(((b0 + 1ull) / 7ull) & 1ull);
   V6 nx;
   v6_zero(nx);
-  if (nblk > 1ull) nx = v6_ldg(is_block_move<kStride>(rows, dig, b0 + 1ull));
-  unsigned long long i = 0;
-  for (; i < nblk; ++i) {
-    const unsigned long long b = b0 + i;
+  if (n > 1) nx = v6_ldg(is_block_move<kStride>(rows, dig, b0 + 1ull));
+  int i = 0;
+  for (; i < n; ++i) {
     if (i) {
       // digits 2.. move to block b, digit 1 returns to alpha^0
       Pl3 d = pl3_lo(nx);
@@ -680,22 +711,40 @@ __device__ __forceinline__ unsigned long long is_walk_blocks(
       qh0 ^= nx.h0;
       qh1 ^= nx.h1;
       qh2 ^= nx.h2;
-      if (i + 1ull < nblk) nx = v6_ldg(is_block_move<kStride>(rows, dig, b + 1ull));
+      if (++m7 == 7) {
+        m7 = 0;
+        par ^= 1;
+      }
+      if (i + 1 < n) {
+        const V6* mv = m7 != 0 ? rows + dig[0] + 1 + (par ? 6 - m7 : m7 - 1)
+                               : is_block_move<kStride>(rows, dig, b0 + unsigned(i) + 1ull);
+        nx = v6_ldg(mv);
+      }
     }
-    // sweep s at digit-1 coefficient alpha^s; alpha^0..6 = 1, 2, 4, 3, 6, 7, 5
-    TG_IS_SWEEP(1u); TG_IS_MOVE(0); TG_IS_SWEEP(2u); TG_IS_MOVE(1); TG_IS_SWEEP(4u);
-    TG_IS_MOVE(2); TG_IS_SWEEP(3u); TG_IS_MOVE(3); TG_IS_SWEEP(6u); TG_IS_MOVE(4);
-    TG_IS_SWEEP(7u); TG_IS_MOVE(5); TG_IS_SWEEP(5u);
+    // Sweep s at digit-1 coefficient alpha^s; alpha^0..6 = 1, 2, 4, 3, 6, 7, 5.
+    // The pair test pays once thr >= kIsPairThr: below it a pair's count
+    // passes thr so often that the exact path costs more than it saves.
+    if (thz + ngz >= kIsPairThr) {
+      TG_IS_SWEEP2(1u); TG_IS_MOVE(0); TG_IS_SWEEP2(2u); TG_IS_MOVE(1); TG_IS_SWEEP2(4u);
+      TG_IS_MOVE(2); TG_IS_SWEEP2(3u); TG_IS_MOVE(3); TG_IS_SWEEP2(6u); TG_IS_MOVE(4);
+      TG_IS_SWEEP2(7u); TG_IS_MOVE(5); TG_IS_SWEEP2(5u);
+    } else {
+      TG_IS_SWEEP1(1u); TG_IS_MOVE(0); TG_IS_SWEEP1(2u); TG_IS_MOVE(1); TG_IS_SWEEP1(4u);
+      TG_IS_MOVE(2); TG_IS_SWEEP1(3u); TG_IS_MOVE(3); TG_IS_SWEEP1(6u); TG_IS_MOVE(4);
+      TG_IS_SWEEP1(7u); TG_IS_MOVE(5); TG_IS_SWEEP1(5u);
+    }
     if (wmin < wthr) break;
     // Another task's witness (a weight below wthr) stops the code; with
     // wthr <= 1 there is none, and the flag is not polled.
-    if (wthr > 1 && (i & 15ull) == 15ull && ld_flag(stop)) break;
+    if (wthr > 1 && (i & 15) == 15 && ld_flag(stop)) break;
   }
-  return 49ull * (min(i, nblk - 1ull) + 1ull);
+  return 49ull * static_cast<unsigned long long>(min(i, n - 1) + 1);
 }
 
 #undef TG_IS_MOVE
-#undef TG_IS_SWEEP
+#undef TG_IS_SWEEP2
+#undef TG_IS_SWEEP1
+#undef TG_IS_ZCOUNTS
 
 // Units [u0, u1) of code c at level w (flat over set, support, block); the
 // smallest weight met (or wmin when none is smaller), and the codewords
