@@ -461,8 +461,15 @@ __device__ __forceinline__ void v6_alpha_pow(V6& p, int e) {
 // Gray value of digit 2 + i at the start of block b: the base-7 digit o_i of
 // b, reflected (6 - o_i) when the digits above it sum to an odd number.
 __device__ __forceinline__ int is_block_digit(unsigned long long& rest) {
-  const int o = int(rest % 7ull);
-  rest /= 7ull;
+  int o;
+  if ((rest >> 32) == 0ull) {  // 32-bit arithmetic whenever it fits (w <= 14)
+    const uint32_t r = uint32_t(rest);
+    o = int(r % 7u);
+    rest = r / 7u;
+  } else {
+    o = int(rest % 7ull);
+    rest /= 7ull;
+  }
   return (rest & 1ull) ? 6 - o : o;
 }
 
@@ -766,10 +773,19 @@ __device__ __forceinline__ int is_walk_units(const DistArgs& a,
   ncw = 0ull;
   unsigned long long u = u0;
   while (u < u1) {
-    const unsigned long long j = u / per_set;
-    const unsigned long long r = u - j * per_set;
-    const unsigned long long s = r / bps;
-    const unsigned long long b = r - s * bps;
+    unsigned long long j, s, b;
+    if (((u | per_set) >> 32) == 0ull) {  // 32-bit divisions whenever they fit
+      const uint32_t u32 = uint32_t(u), ps = uint32_t(per_set), bp = uint32_t(bps);
+      const uint32_t j32 = u32 / ps, r32 = u32 - j32 * ps, s32 = r32 / bp;
+      j = j32;
+      s = s32;
+      b = r32 - s32 * bp;
+    } else {
+      j = u / per_set;
+      const unsigned long long r = u - j * per_set;
+      s = r / bps;
+      b = r - s * bps;
+    }
     const unsigned long long nblk = min(bps - b, u1 - u);
     const V6* rows = base + size_t(j) * k * kIsVecPerRow;
     // Support rows from the largest down (combinadic unranking).  The q-th
@@ -832,6 +848,7 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) walk_level_kernel(DistArgs a
   __shared__ unsigned long long s_binom[kIsBinom][kIsBinom];
   __shared__ uint16_t s_dig[kIsMaxDigits][kTPB];
   __shared__ uint32_t s_ez[39][kTPB];
+  if (a.is_hdr->total == 0ull) return;  // no set needs this level (uniform per block)
   for (int i = threadIdx.x; i < kIsBinom * kIsBinom; i += kTPB)
     s_binom[i / kIsBinom][i % kIsBinom] = c_binom[i / kIsBinom][i % kIsBinom];
   __syncthreads();
