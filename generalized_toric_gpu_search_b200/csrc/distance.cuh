@@ -23,7 +23,7 @@ struct IsHeader {
   unsigned long long tasks_all;  // tasks over all levels walked
   unsigned long long codewords;  // codewords evaluated
   int32_t level;
-  int32_t pad;
+  int32_t work;                  // set by plan_level_kernel when some set needs the level
 };
 
 // Per-code descriptor written by the prep kernels.

@@ -320,10 +320,10 @@ __device__ __forceinline__ unsigned long long is_max_task_units(int w) {
 // the units of level w of those that are not.
 __global__ void plan_level_kernel(DistArgs a, int w) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= a.n) return;
   unsigned long long units = 0ull;
-  const CodeDesc d = a.desc[c];
-  if ((d.flags & kIsCodeFlag) != 0 && (d.flags & kDecidedFlag) == 0 && a.abort[c] == 0) {
+  const CodeDesc d = c < a.n ? a.desc[c] : CodeDesc{};
+  if (c < a.n && (d.flags & kIsCodeFlag) != 0 && (d.flags & kDecidedFlag) == 0 &&
+      a.abort[c] == 0) {
     const int best = a.is_best[c];
     const int L = w - 1;
     const int bound = (d.flags & kTorusBoundFlag)
@@ -335,7 +335,9 @@ __global__ void plan_level_kernel(DistArgs a, int w) {
       units = static_cast<unsigned long long>(d.H) * c_binom[d.k][w] * is_units_per_support(w);
     }
   }
-  a.is_units[c] = units;
+  if (c < a.n) a.is_units[c] = units;
+  // Lets scan_level_kernel and walk_level_kernel skip a level no set needs.
+  if (__any_sync(0xffffffffu, units != 0ull) && (threadIdx.x & 31) == 0) a.is_hdr->work = 1;
 }
 
 // Task size of level w (units per task, sized so the level has about eight
@@ -347,6 +349,15 @@ __global__ void __launch_bounds__(kScanThreads) scan_level_kernel(DistArgs a, in
   const int t = threadIdx.x;
   const int lane = t & 31, wid = t >> 5;
   const int n = a.n;
+  if (a.is_hdr->work == 0) {  // written by plan_level_kernel; the same for every thread
+    if (t == 0) {
+      a.is_hdr->counter = 0ull;
+      a.is_hdr->total = 0ull;
+      a.is_hdr->units = 1ull;
+      a.is_hdr->level = w;
+    }
+    return;
+  }
   if (t == 0) s_over = 0;
   __syncthreads();
   const int chunk = (n + kScanThreads - 1) / kScanThreads;
@@ -435,6 +446,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_level_kernel(DistArgs a, in
     a.is_hdr->units = nb;
     a.is_hdr->level = w;
     a.is_hdr->tasks_all += total;
+    a.is_hdr->work = 0;  // every thread read it before the first barrier
   }
 }
 
