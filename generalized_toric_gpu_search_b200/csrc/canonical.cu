@@ -15,7 +15,9 @@
 // matrices l, l + 32, ...: it maps the mask point by point, then for every
 // point q of the image translates the image by -q on the torus Z_7^2
 // (a per-row 7-bit rotation followed by a 49-bit rotation by 7 rows) and keeps
-// the smallest mask.  A 64-bit warp min-reduction finishes the set.
+// the smallest mask, skipping the translations whose top row already exceeds
+// the best (canon_mask_warp_min in common.cuh).  A 64-bit warp min-reduction
+// finishes the set.
 #include "common.cuh"
 #include "canonical.cuh"
 
@@ -81,30 +83,7 @@ __global__ void __launch_bounds__(kCanonTPB, 2) canon_kernel(CanonArgs a) {
       }
       continue;
     }
-    uint64_t best = ~0ull;
-    for (int A = lane; A < kGl2Order; A += 32) {
-      const uint8_t* P = s_perm + A * kN;
-      uint64_t img = 0ull;
-      uint64_t x = S;
-      while (x) {
-        const int p = __ffsll(static_cast<long long>(x)) - 1;
-        x &= x - 1ull;
-        img |= 1ull << P[p];
-      }
-      uint64_t y = img;
-      while (y) {
-        const int q = __ffsll(static_cast<long long>(y)) - 1;
-        y &= y - 1ull;
-        const int qa = (q * 37) >> 8;  // q / 7 for q < 49
-        const int qb = q - 7 * qa;
-        const uint64_t cand = torus_shift(img, qa, qb);
-        best = cand < best ? cand : best;
-      }
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-      const uint64_t other = __shfl_xor_sync(0xffffffffu, best, o);
-      best = other < best ? other : best;
-    }
+    const uint64_t best = canon_mask_warp_min<false>(lane, S, s_perm);
     if (lane == 0) {
       a.out_mask[s] = best;
       uint64_t lo, hi;

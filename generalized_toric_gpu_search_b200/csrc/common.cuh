@@ -166,6 +166,76 @@ __device__ __forceinline__ uint64_t torus_shift(uint64_t m, int qa, int qb) {
   return ((cr >> r) | (cr << (kN - r))) & kMask49;
 }
 
+// Top row of a nonempty 49-bit mask (the highest row of Z_7^2 it occupies)
+// and that row's 7 bits.
+__device__ __forceinline__ void mask_top_row(uint64_t m, int& t, uint32_t& bits) {
+  t = ((63 - __clzll(static_cast<long long>(m))) * 37) >> 8;  // (highest bit) / 7
+  bits = uint32_t(m >> (7 * t)) & 0x7Fu;
+}
+
+// AGL2(F7) canonical mask of S != 0 (the smallest mask among the images of S
+// that contain the origin), by one warp: lane l maps S by the matrices l, l + 32,
+// ... of the GL2 point table `perm` (2016 rows of 49 bytes; read through the
+// read-only path when kLdg), then translates each image by -q for every point
+// q of it.  A candidate's order is decided first by its top row and then by
+// that row's bits, which follow from the image's row occupancy R and one row
+// of the image, so candidates above the best so far are skipped without the
+// full translation.  The lanes share their best every 8 matrices.  Returns the
+// mask in every lane.
+template <bool kLdg>
+__device__ __forceinline__ uint64_t canon_mask_warp_min(int lane, uint64_t S,
+                                                         const uint8_t* perm) {
+  uint64_t best = ~0ull;
+  int tb = 9;           // best's top row (9: none yet)
+  uint32_t pb = 0x7Fu;  // best's top-row bits
+  for (int A = lane, it = 0; A < kGl2Order; A += 32, ++it) {
+    const uint8_t* P = perm + A * kN;
+    uint64_t img = 0ull;
+    uint32_t R = 0u;
+    uint64_t x = S;
+    while (x) {
+      const int p = __ffsll(static_cast<long long>(x)) - 1;
+      x &= x - 1ull;
+      const int idx = kLdg ? __ldg(P + p) : P[p];
+      img |= 1ull << idx;
+      R |= 1u << ((idx * 37) >> 8);  // row idx / 7
+    }
+    uint64_t y = img;
+    while (y) {
+      const int q = __ffsll(static_cast<long long>(y)) - 1;
+      y &= y - 1ull;
+      const int qa = (q * 37) >> 8;  // q / 7 for q < 49
+      const int qb = q - 7 * qa;
+      const uint32_t rr = ((R >> qa) | (R << (7 - qa))) & 0x7Fu;  // rows after the shift
+      const int t = 31 - __clz(rr);
+      if (t > tb) continue;
+      if (t == tb) {
+        int ra = qa + t;
+        ra = ra >= 7 ? ra - 7 : ra;
+        const uint32_t rb = uint32_t(img >> (7 * ra)) & 0x7Fu;
+        if ((((rb >> qb) | (rb << (7 - qb))) & 0x7Fu) > pb) continue;
+      }
+      const uint64_t cand = torus_shift(img, qa, qb);
+      if (cand < best) {
+        best = cand;
+        mask_top_row(best, tb, pb);
+      }
+    }
+    if ((it & 7) == 7 || A + 32 >= kGl2Order) {  // every lane runs 63 matrices
+      uint64_t m = best;
+      for (int o = 16; o > 0; o >>= 1) {
+        const uint64_t other = __shfl_xor_sync(0xffffffffu, m, o);
+        m = other < m ? other : m;
+      }
+      if (m < best) {
+        best = m;
+        mask_top_row(best, tb, pb);
+      }
+    }
+  }
+  return best;
+}
+
 __device__ __forceinline__ void key_from_mask(uint64_t m, uint64_t& lo, uint64_t& hi) {
   const int k = __popcll(m);
   if (k < 1 || k > 16) {

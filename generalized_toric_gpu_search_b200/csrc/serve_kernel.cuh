@@ -67,30 +67,7 @@ __device__ __forceinline__ unsigned long long ent_pack(unsigned int st, int mz, 
 // AGL2(F7) canonical mask of S (popcount >= 1), computed by one warp with the
 // GL2 point table read through L1 (the anchored minimum of canonical.cu).
 __device__ uint64_t canon_mask_warp(int lane, uint64_t S, const uint8_t* gl2) {
-  uint64_t best = ~0ull;
-  for (int A = lane; A < kGl2Order; A += 32) {
-    const uint8_t* P = gl2 + A * kN;
-    uint64_t img = 0ull;
-    uint64_t x = S;
-    while (x) {
-      const int p = __ffsll(static_cast<long long>(x)) - 1;
-      x &= x - 1ull;
-      img |= 1ull << __ldg(P + p);
-    }
-    uint64_t y = img;
-    while (y) {
-      const int q = __ffsll(static_cast<long long>(y)) - 1;
-      y &= y - 1ull;
-      const int qa = (q * 37) >> 8;
-      const uint64_t cand = torus_shift(img, qa, q - 7 * qa);
-      best = cand < best ? cand : best;
-    }
-  }
-  for (int o = 16; o > 0; o >>= 1) {
-    const uint64_t other = __shfl_xor_sync(0xffffffffu, best, o);
-    best = other < best ? other : best;
-  }
-  return best;
+  return canon_mask_warp_min<true>(lane, S, gl2);
 }
 
 // Writes the final answer of a request to host-mapped memory and frees the
