@@ -576,8 +576,7 @@ __device__ __forceinline__ void gf8_scale32(uint32_t c, uint32_t& x0, uint32_t& 
 // sweep's zero counts z[v] (plus zz, the zeros on g's zero columns); the high
 // half is rebuilt from Ph, P's high word without digit 1's term, plus kC r1
 // (kC = digit 1's coefficient in this sweep).
-template <uint32_t kC>
-__device__ __forceinline__ int is_sweep_fix(const int (&z)[7], int zz, uint32_t ph0,
+__device__ __forceinline__ int is_sweep_fix(uint32_t kC, const int (&z)[7], int zz, uint32_t ph0,
                                             uint32_t ph1, uint32_t ph2, const V6* g_row,
                                             const V6* r1_row, int wmin) {
   uint32_t d0 = __ldg(&r1_row->h0), d1 = __ldg(&r1_row->h1), d2 = __ldg(&r1_row->h2);
@@ -617,21 +616,27 @@ __device__ __forceinline__ int is_sweep_fix(const int (&z)[7], int zz, uint32_t 
   z_[4] = __popc(lop3<sel_lut(6)>(W.x0, W.x1, W.x2));                                            \
   z_[5] = __popc(lop3<sel_lut(7)>(W.x0, W.x1, W.x2));                                            \
   z_[6] = __popc(lop3<sel_lut(5)>(W.x0, W.x1, W.x2));
-#define TG_IS_SWEEP1(kC)                                                                         \
+// Sweep S of a block (digit 1 at alpha^S, alpha^0..6 = 1, 2, 4, 3, 6, 7, 5 =
+// kC): a sweep that may hold a codeword lighter than wmin is counted exactly
+// on the spot.  This form serves low thresholds, where that happens often.
+#define TG_IS_SWEEP1(S, kC)                                                                      \
   {                                                                                              \
     TG_IS_ZCOUNTS(z_)                                                                            \
     const int pz_ = __popc(lop3<0xFE>(Pz.x0, Pz.x1, Pz.x2));                                    \
     const int zm_ = __vimax3_s32(__vimax3_s32(z_[0], z_[1], z_[2]),                              \
                                  __vimax3_s32(z_[3], z_[4], z_[5]), z_[6]) - pz_;                \
     if (__builtin_expect(zm_ > thz, 0)) {                                                        \
-      wmin = is_sweep_fix<kC>(z_, ngz - pz_, qh0, qh1, qh2, rows + r0, rows + r1, wmin);         \
+      wmin = is_sweep_fix(kC, z_, ngz - pz_, qh0, qh1, qh2, rows + r0, rows + r1, wmin);         \
       thz = thz_base - wmin;                                                                     \
     }                                                                                            \
   }
 // The same test on pairs of codewords: the selections of alpha^0|alpha^1,
 // alpha^2|alpha^3 and alpha^4|alpha^5 are disjoint, so each pair's count
-// bounds both of its codewords' zeros; four counts instead of seven.
-#define TG_IS_SWEEP2(kC)                                                                         \
+// bounds both of its codewords' zeros; four counts instead of seven.  Used at
+// high thresholds, where flags are rare: bit S of fl marks the sweep, and the
+// block's flagged sweeps are counted after it, so the seven sweeps are one
+// stretch of straight-line code.
+#define TG_IS_SWEEP2(S)                                                                          \
   {                                                                                              \
     const int y0_ = __popc(lop3<sel_lut(1) | sel_lut(2)>(W.x0, W.x1, W.x2));                     \
     const int y1_ = __popc(lop3<sel_lut(4) | sel_lut(3)>(W.x0, W.x1, W.x2));                     \
@@ -639,11 +644,7 @@ __device__ __forceinline__ int is_sweep_fix(const int (&z)[7], int zz, uint32_t 
     const int y3_ = __popc(lop3<sel_lut(5)>(W.x0, W.x1, W.x2));                                  \
     const int pz_ = __popc(lop3<0xFE>(Pz.x0, Pz.x1, Pz.x2));                                    \
     const int ym_ = __vimax3_s32(y0_, y1_, max(y2_, y3_)) - pz_;                                 \
-    if (__builtin_expect(ym_ > thz, 0)) {                                                        \
-      TG_IS_ZCOUNTS(z_)                                                                          \
-      wmin = is_sweep_fix<kC>(z_, ngz - pz_, qh0, qh1, qh2, rows + r0, rows + r1, wmin);         \
-      thz = thz_base - wmin;                                                                     \
-    }                                                                                            \
+    fl |= ym_ > thz ? (1u << (S)) : 0u;                                                          \
   }
 #define TG_IS_MOVE(I)                                                        \
   {                                                                          \
@@ -654,6 +655,34 @@ __device__ __forceinline__ int is_sweep_fix(const int (&z)[7], int zz, uint32_t 
     Pz.x1 ^= ez[(6 * (I) + 4) * kStride];                                    \
     Pz.x2 ^= ez[(6 * (I) + 5) * kStride];                                    \
   }
+
+// The rare path of a block: the sweeps flagged in fl are counted exactly.
+// W and Pz are the state of sweep 6; stepping back through digit 1's moves
+// (ez, stride kStride) gives each earlier sweep's.  Sweep s has digit 1 at
+// alpha^s (alpha^0..6 = 1, 2, 4, 3, 6, 7, 5, packed in nibbles).
+template <int kStride>
+__device__ __forceinline__ int is_block_fix(unsigned fl, Pl3 W, Pl3 Pz, const uint32_t* ez, int ngz,
+                                         uint32_t qh0, uint32_t qh1, uint32_t qh2,
+                                         const V6* g_row, const V6* r1_row, int wmin) {
+  for (int s = 6; s >= 0 && fl != 0u; --s) {
+    if ((fl >> s) & 1u) {
+      TG_IS_ZCOUNTS(z_)
+      const int pz_ = __popc(lop3<0xFE>(Pz.x0, Pz.x1, Pz.x2));
+      wmin = is_sweep_fix((0x05763421u >> (4 * s)) & 0xFu, z_, ngz - pz_, qh0, qh1, qh2, g_row,
+                          r1_row, wmin);
+      fl &= ~(1u << s);
+    }
+    if (s > 0) {
+      W.x0 ^= ez[(6 * (s - 1) + 0) * kStride];
+      W.x1 ^= ez[(6 * (s - 1) + 1) * kStride];
+      W.x2 ^= ez[(6 * (s - 1) + 2) * kStride];
+      Pz.x0 ^= ez[(6 * (s - 1) + 3) * kStride];
+      Pz.x1 ^= ez[(6 * (s - 1) + 4) * kStride];
+      Pz.x2 ^= ez[(6 * (s - 1) + 5) * kStride];
+    }
+  }
+  return wmin;
+}
 
 // Smallest thr at which a block is tested on pairs of codewords (with seven
 // selections of about 7/64 of the 32 low columns each, a pair's count tops 15
@@ -740,17 +769,23 @@ __device__ __forceinline__ unsigned long long is_walk_blocks(
         nx = v6_ldg(mv);
       }
     }
-    // Sweep s at digit-1 coefficient alpha^s; alpha^0..6 = 1, 2, 4, 3, 6, 7, 5.
+    // Sweep s at digit-1 coefficient alpha^s; the flagged ones are counted
+    // exactly after the block.
     // The pair test pays once thr >= kIsPairThr: below it a pair's count
     // passes thr so often that the exact path costs more than it saves.
+    unsigned fl = 0u;
     if (thz + ngz >= kIsPairThr) {
-      TG_IS_SWEEP2(1u); TG_IS_MOVE(0); TG_IS_SWEEP2(2u); TG_IS_MOVE(1); TG_IS_SWEEP2(4u);
-      TG_IS_MOVE(2); TG_IS_SWEEP2(3u); TG_IS_MOVE(3); TG_IS_SWEEP2(6u); TG_IS_MOVE(4);
-      TG_IS_SWEEP2(7u); TG_IS_MOVE(5); TG_IS_SWEEP2(5u);
+      TG_IS_SWEEP2(0); TG_IS_MOVE(0); TG_IS_SWEEP2(1); TG_IS_MOVE(1); TG_IS_SWEEP2(2);
+      TG_IS_MOVE(2); TG_IS_SWEEP2(3); TG_IS_MOVE(3); TG_IS_SWEEP2(4); TG_IS_MOVE(4);
+      TG_IS_SWEEP2(5); TG_IS_MOVE(5); TG_IS_SWEEP2(6);
     } else {
-      TG_IS_SWEEP1(1u); TG_IS_MOVE(0); TG_IS_SWEEP1(2u); TG_IS_MOVE(1); TG_IS_SWEEP1(4u);
-      TG_IS_MOVE(2); TG_IS_SWEEP1(3u); TG_IS_MOVE(3); TG_IS_SWEEP1(6u); TG_IS_MOVE(4);
-      TG_IS_SWEEP1(7u); TG_IS_MOVE(5); TG_IS_SWEEP1(5u);
+      TG_IS_SWEEP1(0, 1u); TG_IS_MOVE(0); TG_IS_SWEEP1(1, 2u); TG_IS_MOVE(1); TG_IS_SWEEP1(2, 4u);
+      TG_IS_MOVE(2); TG_IS_SWEEP1(3, 3u); TG_IS_MOVE(3); TG_IS_SWEEP1(4, 6u); TG_IS_MOVE(4);
+      TG_IS_SWEEP1(5, 7u); TG_IS_MOVE(5); TG_IS_SWEEP1(6, 5u);
+    }
+    if (__builtin_expect(fl != 0u, 0)) {
+      wmin = is_block_fix<kStride>(fl, W, Pz, ez, ngz, qh0, qh1, qh2, rows + r0, rows + r1, wmin);
+      thz = thz_base - wmin;
     }
     if (wmin < wthr) break;
     // Another task's witness (a weight below wthr) stops the code; with
