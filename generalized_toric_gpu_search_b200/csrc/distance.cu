@@ -889,10 +889,11 @@ int run_walk(const DistArgs& args, int sm_count, int blocks_per_sm, int tpb, cud
   }
   if (e != cudaSuccess) return cuda_fail(e, "walk kernel launch");
   if ((parts & kWalkInfoset) && args.is_min_k <= args.k_max) {
-    // Information-set walk, one level per launch triple; 6 CTAs of 128
-    // threads per SM (80 registers, 27 KB of shared memory each).  Levels no
-    // code needs find no tasks.
-    constexpr int kPerSm = 6;
+    // Information-set walk, one level per launch triple; 5 CTAs of 128
+    // threads per SM (96 registers, no spills, 28 KB of shared memory each;
+    // 6 CTAs at 80 registers spill and ran 1 % slower).  Levels no code needs
+    // return before any setup.
+    constexpr int kPerSm = 5;
     DistArgs la = args;
     la.is_lanes = sm_count * kPerSm * kIsWalkThreads;
     const int plan_grid = (args.n + 255) / 256;
