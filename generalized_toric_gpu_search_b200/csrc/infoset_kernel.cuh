@@ -711,16 +711,22 @@ __device__ __forceinline__ unsigned long long is_walk_blocks(
   const Pl3 h = pl3_inv(g);
   const uint32_t gz = ~(g.x0 | g.x1 | g.x2);  // low columns where g is 0
   const int ngz = __popc(gz);
+  // Digit 1's step i is (alpha^i + alpha^(i+1)) r1 = alpha^i (1 + alpha) r1:
+  // one product with h for the first, then a multiplication by alpha (one
+  // XOR) for each next, in both domains.
+  const Pl3 d0 = pl3_lo(v6_ldg(rows + r1 + 1));
+  Pl3 e = pl3_mul(d0, h);
+  Pl3 zq = pl3_and(d0, gz);
 #pragma unroll
   for (int i = 0; i < 6; ++i) {
-    const Pl3 d = pl3_lo(v6_ldg(rows + r1 + 1 + i));
-    const Pl3 e = pl3_mul(d, h);
     ez[(6 * i + 0) * kStride] = e.x0;
     ez[(6 * i + 1) * kStride] = e.x1;
     ez[(6 * i + 2) * kStride] = e.x2;
-    ez[(6 * i + 3) * kStride] = d.x0 & gz;
-    ez[(6 * i + 4) * kStride] = d.x1 & gz;
-    ez[(6 * i + 5) * kStride] = d.x2 & gz;
+    ez[(6 * i + 3) * kStride] = zq.x0;
+    ez[(6 * i + 4) * kStride] = zq.x1;
+    ez[(6 * i + 5) * kStride] = zq.x2;
+    e = Pl3{e.x2, e.x0 ^ e.x2, e.x1};  // alpha e
+    zq = Pl3{zq.x2, zq.x0 ^ zq.x2, zq.x1};
   }
   {
     // (alpha^6 + alpha^0) r1 = alpha^2 r1
