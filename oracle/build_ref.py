@@ -9,8 +9,8 @@ modules from the reference checkout with `cupy` and `pyopencl` stubbed (the
 modules only touch them inside methods), writes the two strings unchanged to
 oracle/_ref/, and compiles them with nvcc for sm_100a together with
 oracle/ref_harness.cu into oracle/_ref/libref_kernels.so.  oracle/_ref/ is
-git-ignored (nothing of the reference is committed) and travels to the GPU box
-with the rest of the working tree.
+git-ignored (nothing of the reference is committed); a copy of the working tree
+taken to a machine without the reference checkout carries the built library.
 
 Usage: python oracle/build_ref.py [--reference /root/reference]
 """
@@ -57,7 +57,7 @@ def extract_sources(reference: Path) -> dict[str, str]:
 
 def build(reference: Path = DEFAULT_REFERENCE, force: bool = False) -> Path | None:
     """Builds oracle/_ref/libref_kernels.so; returns None when the reference
-    checkout is absent (the GPU box uses the prebuilt library)."""
+    checkout is absent (a machine without it uses the prebuilt library)."""
     if not (reference / "kernel_cuda_bp.py").exists():
         return LIB if LIB.exists() else None
     harness = ORACLE_DIR / "ref_harness.cu"

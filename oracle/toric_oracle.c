@@ -1,7 +1,8 @@
 /*
  * ORACLE — test infrastructure only.  CPU restatement of the reference's
  * algorithms for the GF(8) toric-code hot path, used by tests/, by
- * __graft_entry__.smoke() as the checker and by bench.py's CPU-baseline leg.
+ * __graft_entry__.smoke() to check the device results and by bench.py's
+ * CPU-baseline leg.
  * The product (generalized_toric_gpu_search_b200) never links or calls it.
  *
  * Restated from (paths inside the reference project):
