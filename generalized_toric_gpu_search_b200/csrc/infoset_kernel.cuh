@@ -974,6 +974,49 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) walk_level_kernel(DistArgs a
   if (lane == 0 && evaluated) atomicAdd(&a.is_hdr->codewords, evaluated);
 }
 
+// Levels 1 and 2 of every set in one launch, one warp per set: the rows
+// themselves (weight-1 messages) and, for each pair of rows q < p, the sweep
+// alpha^v row_p + row_q (weight-2 messages up to scalars).  These levels are
+// too small to fill the GPU one at a time, and running level 2 without first
+// checking the bound after level 1 only adds codewords (the best weight stays
+// that of a codeword); level 3 onwards then follows the plan / scan / walk
+// triple.
+__global__ void __launch_bounds__(128) levels12_kernel(DistArgs a) {
+  const int lane = threadIdx.x & 31;
+  const int c = blockIdx.x * 4 + (threadIdx.x >> 5);
+  if (c >= a.n) return;  // warp-uniform
+  const CodeDesc d = a.desc[c];
+  if ((d.flags & kIsCodeFlag) == 0 || (d.flags & kDecidedFlag) != 0 || ld_flag(a.abort + c) != 0)
+    return;
+  const int k = d.k;
+  const int n1 = k, per_set = k + k * (k - 1) / 2;
+  const int total = d.H * per_set;
+  const V6* base = a.is_rows + size_t(c) * a.is_stride;
+  int wmin = kN + 1;
+  for (int u = lane; u < total; u += 32) {
+    const int j = u / per_set;
+    const int r = u - j * per_set;
+    const V6* rows = base + size_t(j) * k * kIsVecPerRow;
+    if (r < n1) {
+      const V6 P = v6_ldg(rows + r * kIsVecPerRow);
+      wmin = min(wmin, __popc(lop3<0xFE>(P.l0, P.l1, P.l2)) + __popc(lop3<0xFE>(P.h0, P.h1, P.h2)));
+    } else {
+      const int r2 = r - n1;  // pair (q, p), q < p: p(p-1)/2 <= r2 < p(p+1)/2
+      int p = 1;
+      while ((p + 1) * p / 2 <= r2) ++p;
+      const int q = r2 - p * (p - 1) / 2;
+      wmin = is_sweep_exact(v6_ldg(rows + q * kIsVecPerRow), rows + p * kIsVecPerRow, wmin);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) wmin = min(wmin, __shfl_xor_sync(0xffffffffu, wmin, o));
+  if (lane == 0) {
+    atomicAdd(&a.is_hdr->codewords,
+              static_cast<unsigned long long>(d.H) * static_cast<unsigned long long>(k + 7 * (per_set - k)));
+    if (wmin < a.is_best[c]) a.is_best[c] = wmin;
+    if (a.is_best[c] < kN - d.tmax) a.abort[c] = 1;  // a witness below the target distance
+  }
+}
+
 __global__ void finalize_infoset_kernel(DistArgs a) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= a.n) return;
