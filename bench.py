@@ -59,10 +59,10 @@ ENUMERATIONS = {
 
 def launches_per_step(k_max: int, enumeration: str) -> int:
     """Kernels per step: prep_exact, scan_tasks and the enumeration walk; with
-    information sets also prep_infoset, levels12 (levels 1 and 2), per level
-    3..k_max plan, scan and walk, and finalize_infoset."""
+    information sets also prep_infoset, levels123 (levels 1 to 3), per level
+    4..k_max plan, scan and walk, and finalize_infoset."""
     infoset = enumeration == "infoset" or (enumeration == "auto" and k_max >= 10)
-    return 3 + ((3 + 3 * max(0, k_max - 2)) if infoset else 0)
+    return 3 + ((3 + 3 * max(0, k_max - 3)) if infoset else 0)
 
 
 L2_FLUSH_BYTES = 256 << 20

@@ -897,8 +897,8 @@ int run_walk(const DistArgs& args, int sm_count, int blocks_per_sm, int tpb, cud
     DistArgs la = args;
     la.is_lanes = sm_count * kPerSm * kIsWalkThreads;
     const int plan_grid = (args.n + 255) / 256;
-    levels12_kernel<<<(args.n + 3) / 4, 128, 0, s>>>(la);
-    for (int w = 3; w <= args.k_max; ++w) {
+    levels123_kernel<<<(args.n + 3) / 4, 128, 0, s>>>(la);
+    for (int w = 4; w <= args.k_max; ++w) {
       plan_level_kernel<<<plan_grid, 256, 0, s>>>(la, w);
       scan_level_kernel<<<1, kScanThreads, 0, s>>>(la, w);
       walk_level_kernel<kIsWalkThreads, kPerSm><<<sm_count * kPerSm, kIsWalkThreads, 0, s>>>(la, w);

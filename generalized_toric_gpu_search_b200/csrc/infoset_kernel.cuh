@@ -974,14 +974,15 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) walk_level_kernel(DistArgs a
   if (lane == 0 && evaluated) atomicAdd(&a.is_hdr->codewords, evaluated);
 }
 
-// Levels 1 and 2 of every set in one launch, one warp per set: the rows
-// themselves (weight-1 messages) and, for each pair of rows q < p, the sweep
-// alpha^v row_p + row_q (weight-2 messages up to scalars).  These levels are
-// too small to fill the GPU one at a time, and running level 2 without first
-// checking the bound after level 1 only adds codewords (the best weight stays
-// that of a codeword); level 3 onwards then follows the plan / scan / walk
-// triple.
-__global__ void __launch_bounds__(128) levels12_kernel(DistArgs a) {
+// Levels 1 to 3 of every set in one launch, one warp per set: the rows
+// themselves (weight-1 messages); for each pair of rows q < p the sweep
+// alpha^v row_p + row_q; and for each triple q < p < t the seven sweeps
+// alpha^v row_t + alpha^s row_p + row_q (messages up to scalars).  These
+// levels are too small to fill the GPU one launch each, and running them
+// without the bound check between them only adds codewords (the best weight
+// stays that of a codeword); level 4 onwards then follows the plan / scan /
+// walk triple.
+__global__ void __launch_bounds__(128) levels123_kernel(DistArgs a) {
   const int lane = threadIdx.x & 31;
   const int c = blockIdx.x * 4 + (threadIdx.x >> 5);
   if (c >= a.n) return;  // warp-uniform
@@ -989,29 +990,48 @@ __global__ void __launch_bounds__(128) levels12_kernel(DistArgs a) {
   if ((d.flags & kIsCodeFlag) == 0 || (d.flags & kDecidedFlag) != 0 || ld_flag(a.abort + c) != 0)
     return;
   const int k = d.k;
-  const int n1 = k, per_set = k + k * (k - 1) / 2;
+  const int n1 = k, n2 = k * (k - 1) / 2, n3 = k * (k - 1) * (k - 2) / 6;
+  const int per_set = n1 + n2 + n3;
   const int total = d.H * per_set;
   const V6* base = a.is_rows + size_t(c) * a.is_stride;
   int wmin = kN + 1;
   for (int u = lane; u < total; u += 32) {
     const int j = u / per_set;
-    const int r = u - j * per_set;
+    int r = u - j * per_set;
     const V6* rows = base + size_t(j) * k * kIsVecPerRow;
     if (r < n1) {
       const V6 P = v6_ldg(rows + r * kIsVecPerRow);
       wmin = min(wmin, __popc(lop3<0xFE>(P.l0, P.l1, P.l2)) + __popc(lop3<0xFE>(P.h0, P.h1, P.h2)));
+      continue;
+    }
+    r -= n1;
+    int t = -1;  // the third row of a triple: C(t, 3) <= r < C(t + 1, 3)
+    if (r >= n2) {
+      r -= n2;
+      t = 2;
+      while ((t + 1) * t * (t - 1) / 6 <= r) ++t;
+      r -= t * (t - 1) * (t - 2) / 6;
+    }
+    int p = 1;  // pair q < p: C(p, 2) <= r < C(p + 1, 2)
+    while ((p + 1) * p / 2 <= r) ++p;
+    const int q = r - p * (p - 1) / 2;
+    const V6 Q = v6_ldg(rows + q * kIsVecPerRow);
+    if (t < 0) {
+      wmin = is_sweep_exact(Q, rows + p * kIsVecPerRow, wmin);
     } else {
-      const int r2 = r - n1;  // pair (q, p), q < p: p(p-1)/2 <= r2 < p(p+1)/2
-      int p = 1;
-      while ((p + 1) * p / 2 <= r2) ++p;
-      const int q = r2 - p * (p - 1) / 2;
-      wmin = is_sweep_exact(v6_ldg(rows + q * kIsVecPerRow), rows + p * kIsVecPerRow, wmin);
+      V6 X = v6_ldg(rows + p * kIsVecPerRow);  // alpha^s row_p, s = 0..6
+      for (int s7 = 0; s7 < 7; ++s7) {
+        V6 P = Q;
+        v6_xor(P, X);
+        wmin = is_sweep_exact(P, rows + t * kIsVecPerRow, wmin);
+        v6_alpha_pow(X, 1);
+      }
     }
   }
   for (int o = 16; o > 0; o >>= 1) wmin = min(wmin, __shfl_xor_sync(0xffffffffu, wmin, o));
   if (lane == 0) {
-    atomicAdd(&a.is_hdr->codewords,
-              static_cast<unsigned long long>(d.H) * static_cast<unsigned long long>(k + 7 * (per_set - k)));
+    atomicAdd(&a.is_hdr->codewords, static_cast<unsigned long long>(d.H) *
+                                        static_cast<unsigned long long>(n1 + 7 * n2 + 49 * n3));
     if (wmin < a.is_best[c]) a.is_best[c] = wmin;
     if (a.is_best[c] < kN - d.tmax) a.abort[c] = 1;  // a witness below the target distance
   }
