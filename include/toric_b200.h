@@ -206,9 +206,9 @@ int tg_distance_counters(const tg_distance_params* p, const void* d_workspace,
                          uint64_t* h_codewords, double* h_reference_messages);
 
 /* The same accounting per walk (synchronises `stream`): h_counts[0..3] =
- * enumeration walk tasks and codewords, information-set tasks queued (every
- * level of every set, most of them skipped once a set is finished) and
- * codewords the information-set walk evaluated. */
+ * enumeration walk tasks and codewords, information-set tasks queued (levels
+ * 4 and up; levels 1-3 run as one warp per set, without tasks) and codewords
+ * the information-set walk evaluated (all levels). */
 int tg_distance_path_counters(const tg_distance_params* p, const void* d_workspace,
                               void* stream, uint64_t* h_counts);
 
