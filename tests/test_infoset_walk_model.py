@@ -121,3 +121,35 @@ def test_digit1_return_is_alpha_squared():
     for a in range(8):
         x0, x1, x2 = a & 1, (a >> 1) & 1, (a >> 2) & 1
         assert (x1 | (x1 ^ x2) << 1 | (x0 ^ x2) << 2) == mul(a, ALPHA[2])
+
+
+def unrank_small_levels(k: int):
+    """Units of levels 1-3 of one set, as levels123_kernel unranks them:
+    rows, then pairs q < p, then triples q < p < t."""
+    n1, n2, n3 = k, k * (k - 1) // 2, k * (k - 1) * (k - 2) // 6
+    out = []
+    for r in range(n1 + n2 + n3):
+        if r < n1:
+            out.append((r,))
+            continue
+        r -= n1
+        t = -1
+        if r >= n2:
+            r -= n2
+            t = 2
+            while (t + 1) * t * (t - 1) // 6 <= r:
+                t += 1
+            r -= t * (t - 1) * (t - 2) // 6
+        p = 1
+        while (p + 1) * p // 2 <= r:
+            p += 1
+        q = r - p * (p - 1) // 2
+        out.append((q, p) if t < 0 else (q, p, t))
+    return out
+
+
+@pytest.mark.parametrize("k", [1, 2, 3, 7, 14, 21])
+def test_levels123_unranking_covers_every_support(k):
+    got = unrank_small_levels(k)
+    want = [c for w in (1, 2, 3) for c in itertools.combinations(range(k), w)]
+    assert sorted(got) == sorted(want) and len(got) == len(want)
