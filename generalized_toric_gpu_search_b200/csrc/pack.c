@@ -3,11 +3,20 @@
  * The reference's oracles take a Python list of index lists
  * (kernel_cuda_bp.py:290-323).  Flattening 10^4-10^5 small lists into the
  * int32 index array and int64 offsets the device path reads is a per-item
- * Python loop; this extension does it in C and hands back the two arrays as
- * bytearrays, which the caller views with numpy without a copy.
+ * Python loop; this extension does it in C.
  *
- *   pack(batch) -> (flat: bytearray of int32, offsets: bytearray of int64, k_max: int,
- *                   bad: bool)
+ *   pack(batch) -> (flat: bytearray of int32, offsets: bytearray of int64,
+ *                   k_max: int, bad: bool)
+ *       hands back the two arrays as bytearrays, which the caller views with
+ *       numpy without a copy.
+ *   pack_into(batch, flat_addr, flat_cap, off_addr, off_cap)
+ *       -> (total: int, k_max: int, bad: bool, done: bool)
+ *       writes the same arrays into caller-owned memory (for instance pinned
+ *       staging buffers that the host-to-device copy reads directly) at the
+ *       given addresses, of flat_cap int32 and off_cap int64 elements.  When
+ *       the batch needs more (total > flat_cap or len(batch) + 1 > off_cap) it
+ *       writes nothing and returns done = False with the sizes in total and
+ *       k_max.
  *
  * batch is a sequence of sequences of ints.  `bad` is True when an index lies
  * outside 0..48; such values are stored as given when they fit int32 and as -1
@@ -17,67 +26,115 @@
 #include <stdint.h>
 #include <string.h>
 
-static PyObject* pack(PyObject* self, PyObject* args) {
-  PyObject* batch;
-  (void)self;
-  if (!PyArg_ParseTuple(args, "O", &batch)) return NULL;
-  PyObject* outer = PySequence_Fast(batch, "batch must be a sequence of index sequences");
-  if (!outer) return NULL;
-  const Py_ssize_t n = PySequence_Fast_GET_SIZE(outer);
-  PyObject** sets = PySequence_Fast_ITEMS(outer);
-  /* first pass: total size (keeps the inner fast sequences) */
-  PyObject** inner = (PyObject**)PyMem_Calloc((size_t)(n > 0 ? n : 1), sizeof(PyObject*));
-  if (!inner) {
-    Py_DECREF(outer);
-    return PyErr_NoMemory();
+/* The batch as fast sequences: outer, and inner[i] for each set (new
+ * references, released by release_batch); total indices and k_max. */
+typedef struct {
+  PyObject* outer;
+  PyObject** inner;
+  Py_ssize_t n, total, k_max;
+} Batch;
+
+static void release_batch(Batch* b) {
+  if (b->inner) {
+    for (Py_ssize_t i = 0; i < b->n; ++i) Py_XDECREF(b->inner[i]);
+    PyMem_Free(b->inner);
   }
-  Py_ssize_t total = 0, k_max = 0;
-  PyObject* result = NULL;
-  for (Py_ssize_t i = 0; i < n; ++i) {
-    inner[i] = PySequence_Fast(sets[i], "every set must be a sequence of indices");
-    if (!inner[i]) goto done;
-    const Py_ssize_t k = PySequence_Fast_GET_SIZE(inner[i]);
-    total += k;
-    if (k > k_max) k_max = k;
+  Py_XDECREF(b->outer);
+}
+
+static int collect_batch(PyObject* batch, Batch* b) {
+  memset(b, 0, sizeof(*b));
+  b->outer = PySequence_Fast(batch, "batch must be a sequence of index sequences");
+  if (!b->outer) return -1;
+  b->n = PySequence_Fast_GET_SIZE(b->outer);
+  PyObject** sets = PySequence_Fast_ITEMS(b->outer);
+  b->inner = (PyObject**)PyMem_Calloc((size_t)(b->n > 0 ? b->n : 1), sizeof(PyObject*));
+  if (!b->inner) {
+    PyErr_NoMemory();
+    return -1;
   }
-  PyObject* flat = PyByteArray_FromStringAndSize(NULL, (total > 0 ? total : 1) * (Py_ssize_t)sizeof(int32_t));
-  PyObject* offs = PyByteArray_FromStringAndSize(NULL, (n + 1) * (Py_ssize_t)sizeof(int64_t));
-  if (!flat || !offs) {
-    Py_XDECREF(flat);
-    Py_XDECREF(offs);
-    goto done;
+  for (Py_ssize_t i = 0; i < b->n; ++i) {
+    b->inner[i] = PySequence_Fast(sets[i], "every set must be a sequence of indices");
+    if (!b->inner[i]) return -1;
+    const Py_ssize_t k = PySequence_Fast_GET_SIZE(b->inner[i]);
+    b->total += k;
+    if (k > b->k_max) b->k_max = k;
   }
-  int32_t* f = (int32_t*)PyByteArray_AS_STRING(flat);
-  int64_t* o = (int64_t*)PyByteArray_AS_STRING(offs);
-  int bad = 0;
+  return 0;
+}
+
+/* Writes the flat indices and offsets; -1 with an exception set when an item
+ * is not an int. */
+static int fill_batch(const Batch* b, int32_t* f, int64_t* o, int* bad) {
   Py_ssize_t pos = 0;
+  *bad = 0;
   o[0] = 0;
-  for (Py_ssize_t i = 0; i < n; ++i) {
-    const Py_ssize_t k = PySequence_Fast_GET_SIZE(inner[i]);
-    PyObject** items = PySequence_Fast_ITEMS(inner[i]);
+  for (Py_ssize_t i = 0; i < b->n; ++i) {
+    const Py_ssize_t k = PySequence_Fast_GET_SIZE(b->inner[i]);
+    PyObject** items = PySequence_Fast_ITEMS(b->inner[i]);
     for (Py_ssize_t j = 0; j < k; ++j) {
       const long v = PyLong_AsLong(items[j]);
-      if (v == -1 && PyErr_Occurred()) {
-        Py_DECREF(flat);
-        Py_DECREF(offs);
-        goto done;
-      }
-      if (v < 0 || v > 48) bad = 1;
+      if (v == -1 && PyErr_Occurred()) return -1;
+      if (v < 0 || v > 48) *bad = 1;
       f[pos++] = (v < INT32_MIN || v > INT32_MAX) ? -1 : (int32_t)v;
     }
     o[i + 1] = (int64_t)pos;
   }
-  if (total == 0) f[0] = 0;
-  result = Py_BuildValue("(NNnO)", flat, offs, k_max, bad ? Py_True : Py_False);
-done:
-  for (Py_ssize_t i = 0; i < n; ++i) Py_XDECREF(inner[i]);
-  PyMem_Free(inner);
-  Py_DECREF(outer);
+  return 0;
+}
+
+static PyObject* pack(PyObject* self, PyObject* args) {
+  PyObject* batch;
+  (void)self;
+  if (!PyArg_ParseTuple(args, "O", &batch)) return NULL;
+  Batch b;
+  PyObject* result = NULL;
+  if (collect_batch(batch, &b) == 0) {
+    PyObject* flat =
+        PyByteArray_FromStringAndSize(NULL, (b.total > 0 ? b.total : 1) * (Py_ssize_t)sizeof(int32_t));
+    PyObject* offs = PyByteArray_FromStringAndSize(NULL, (b.n + 1) * (Py_ssize_t)sizeof(int64_t));
+    int bad = 0;
+    if (flat && offs) {
+      int32_t* f = (int32_t*)PyByteArray_AS_STRING(flat);
+      if (b.total == 0) f[0] = 0;
+      if (fill_batch(&b, f, (int64_t*)PyByteArray_AS_STRING(offs), &bad) == 0) {
+        result = Py_BuildValue("(NNnO)", flat, offs, b.k_max, bad ? Py_True : Py_False);
+        flat = offs = NULL;  /* owned by result */
+      }
+    }
+    Py_XDECREF(flat);
+    Py_XDECREF(offs);
+  }
+  release_batch(&b);
+  return result;
+}
+
+static PyObject* pack_into(PyObject* self, PyObject* args) {
+  PyObject* batch;
+  unsigned long long flat_addr, off_addr;
+  Py_ssize_t flat_cap, off_cap;
+  (void)self;
+  if (!PyArg_ParseTuple(args, "OKnKn", &batch, &flat_addr, &flat_cap, &off_addr, &off_cap))
+    return NULL;
+  Batch b;
+  PyObject* result = NULL;
+  if (collect_batch(batch, &b) == 0) {
+    if (b.total > flat_cap || b.n + 1 > off_cap) {
+      result = Py_BuildValue("(nnOO)", b.total, b.k_max, Py_False, Py_False);
+    } else {
+      int bad = 0;
+      if (fill_batch(&b, (int32_t*)(uintptr_t)flat_addr, (int64_t*)(uintptr_t)off_addr, &bad) == 0)
+        result = Py_BuildValue("(nnOO)", b.total, b.k_max, bad ? Py_True : Py_False, Py_True);
+    }
+  }
+  release_batch(&b);
   return result;
 }
 
 static PyMethodDef kMethods[] = {
     {"pack", pack, METH_VARARGS, "Flattens a batch of index sequences (int32 flat, int64 offsets)."},
+    {"pack_into", pack_into, METH_VARARGS,
+     "Flattens a batch of index sequences into caller-owned int32 / int64 arrays."},
     {NULL, NULL, 0, NULL}};
 
 static struct PyModuleDef kModule = {PyModuleDef_HEAD_INIT, "_pack", NULL, -1, kMethods,

@@ -247,6 +247,39 @@ class DistanceOracleCUDABP:
         self.device = self.runner.device
         self._stream = torch.cuda.Stream(device=self.device)
         self._lock = threading.Lock()
+        # Pinned staging of the packed batch, reused across calls; the event
+        # marks the end of the last call's host-to-device copies out of it.
+        self._h_idx: torch.Tensor | None = None
+        self._h_off: torch.Tensor | None = None
+        self._staged: torch.cuda.Event | None = None
+
+    def _stage(self, batched_indices):
+        """Packs the batch straight into the pinned staging buffers (the C
+        packer); None when the packer is missing or the items are not ints.
+        Returns (h_idx, h_off, k_max, bad) views of the staging buffers."""
+        if _PACKER is None or not hasattr(_PACKER, "pack_into"):
+            return None
+        n = len(batched_indices)
+        if self._staged is not None:
+            self._staged.synchronize()  # the last copies out of the buffers are done
+        if self._h_off is None or self._h_off.numel() < n + 1:
+            self._h_off = torch.empty(max(n + 1, 1 << 12), dtype=torch.int64, pin_memory=True)
+        if self._h_idx is None:
+            self._h_idx = torch.empty(1 << 16, dtype=torch.int32, pin_memory=True)
+        for _ in range(2):
+            try:
+                total, k_max, bad, done = _PACKER.pack_into(
+                    batched_indices, self._h_idx.data_ptr(), self._h_idx.numel(),
+                    self._h_off.data_ptr(), self._h_off.numel())
+            except (TypeError, OverflowError):
+                return None
+            if done:
+                if total == 0:
+                    self._h_idx[0] = 0
+                return self._h_idx[:max(total, 1)], self._h_off[:n + 1], k_max, bad
+            self._h_idx = torch.empty(max(total, 2 * self._h_idx.numel()), dtype=torch.int32,
+                                      pin_memory=True)
+        raise RuntimeError("batch packing did not fit its staging buffer")
 
     def _runner_for(self, k_max: int, sampled: bool) -> DistanceRunner:
         """Launch shape: the fixed config, else the autotuned one for k_max."""
@@ -287,26 +320,35 @@ class DistanceOracleCUDABP:
     # -- implementation -------------------------------------------------------
 
     def _evaluate(self, batched_indices, target_distance, sample_count, sample_seed) -> list[int]:
-        flat, offsets, k_max = pack_sets(batched_indices)
-        if k_max > MAX_SAMPLED_K:
-            raise ValueError("CUDA-BP bit-parallel kernel supports k <= 49")
-        if sample_count <= 0 and k_max > MAX_EXACT_K:
-            raise ValueError("Exact CUDA-BP batch evaluation supports k <= 21")
-        if flat.size and (int(flat.min()) < 0 or int(flat.max()) >= N_POINTS):
-            raise ValueError("exponent indices must lie in 0..48")
         n = len(batched_indices)
-        per_set_td = not np.isscalar(target_distance)
-        td_arr = None
-        if per_set_td:
-            td_arr = np.asarray(target_distance, dtype=np.int32)
-            if td_arr.shape != (n,):
-                raise ValueError("target_distance must be an int or one value per set")
         with self._lock, torch.cuda.device(self.device):
+            staged = self._stage(batched_indices)
+            if staged is None:
+                flat, offsets, k_max = pack_sets(batched_indices)
+                bad = bool(flat.size) and (int(flat.min()) < 0 or int(flat.max()) >= N_POINTS)
+                h_idx = torch.from_numpy(flat if flat.size else np.zeros(1, np.int32)).pin_memory()
+                h_off = torch.from_numpy(offsets).pin_memory()
+            else:
+                h_idx, h_off, k_max, bad = staged
+            if k_max > MAX_SAMPLED_K:
+                raise ValueError("CUDA-BP bit-parallel kernel supports k <= 49")
+            if sample_count <= 0 and k_max > MAX_EXACT_K:
+                raise ValueError("Exact CUDA-BP batch evaluation supports k <= 21")
+            if bad:
+                raise ValueError("exponent indices must lie in 0..48")
+            per_set_td = not np.isscalar(target_distance)
+            td_arr = None
+            if per_set_td:
+                td_arr = np.asarray(target_distance, dtype=np.int32)
+                if td_arr.shape != (n,):
+                    raise ValueError("target_distance must be an int or one value per set")
             s = self._stream
             with torch.cuda.stream(s):
-                d_idx = torch.from_numpy(flat if flat.size else np.zeros(1, np.int32)).pin_memory()
-                d_idx = d_idx.to(self.device, non_blocking=True)
-                d_off = torch.from_numpy(offsets).pin_memory().to(self.device, non_blocking=True)
+                d_idx = h_idx.to(self.device, non_blocking=True)
+                d_off = h_off.to(self.device, non_blocking=True)
+                if self._staged is None:
+                    self._staged = torch.cuda.Event()
+                self._staged.record(s)
                 d_td = None
                 if td_arr is not None:
                     d_td = torch.from_numpy(td_arr).pin_memory().to(self.device, non_blocking=True)
