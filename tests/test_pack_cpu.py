@@ -74,3 +74,30 @@ def test_other_element_types_fall_back(packer, monkeypatch):
     assert flat.tolist() == [1, 2, 3, 4, 5] and off.tolist() == [0, 2, 5] and k == 3
     with pytest.raises(TypeError):
         packer.pack(5)
+
+
+def test_pack_into_caller_buffers(packer):
+    rng = np.random.default_rng(9)
+    batch = [rng.choice(49, size=int(rng.integers(0, 22)), replace=False).tolist()
+             for _ in range(500)]
+    flat_b, off_b, k_max, bad = packer.pack(batch)
+    off_ref = np.frombuffer(off_b, np.int64)
+    total = int(off_ref[-1])
+    f = np.full(total + 5, -7, np.int32)
+    o = np.zeros(len(batch) + 1, np.int64)
+    # too small: nothing written, sizes reported
+    assert packer.pack_into(batch, f.ctypes.data, total - 1, o.ctypes.data, o.size) == (
+        total, k_max, False, False)
+    assert (f == -7).all() and not o.any()
+    assert packer.pack_into(batch, f.ctypes.data, f.size, o.ctypes.data, len(batch)) == (
+        total, k_max, False, False)
+    # enough room: the same arrays as pack()
+    assert packer.pack_into(batch, f.ctypes.data, f.size, o.ctypes.data, o.size) == (
+        total, k_max, bad, True)
+    np.testing.assert_array_equal(f[:total], np.frombuffer(flat_b, np.int32)[:total])
+    np.testing.assert_array_equal(o, off_ref)
+    assert (f[total:] == -7).all()
+    # out-of-range indices are flagged, non-int items raise
+    assert packer.pack_into([[1, 50]], f.ctypes.data, f.size, o.ctypes.data, o.size)[2]
+    with pytest.raises(TypeError):
+        packer.pack_into([[1, "a"]], f.ctypes.data, f.size, o.ctypes.data, o.size)
