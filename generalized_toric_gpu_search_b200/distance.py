@@ -122,6 +122,75 @@ def pack_sets(batched_indices) -> tuple[np.ndarray, np.ndarray, int]:
     return flat, offsets, k_max
 
 
+class PinnedBatchStage:
+    """Pinned host staging of packed batches, reused across calls.
+
+    `pack` writes a batch straight into the pinned buffers with the C packer
+    and returns (h_idx, h_off, k_max, bad) views of them, or None when the
+    packer is missing or the items are not ints (the caller then packs with
+    pack_sets).  After enqueueing the host-to-device copies out of the views,
+    the caller calls `mark(stream)`; the next `pack` waits for those copies
+    before it overwrites the buffers.  Not thread-safe: callers hold a lock.
+    """
+
+    def __init__(self):
+        self.h_idx: torch.Tensor | None = None
+        self.h_off: torch.Tensor | None = None
+        self._copied: torch.cuda.Event | None = None
+
+    def pack(self, batched_indices):
+        if _PACKER is None or not hasattr(_PACKER, "pack_into"):
+            return None
+        n = len(batched_indices)
+        if self._copied is not None:
+            self._copied.synchronize()
+        if self.h_off is None or self.h_off.numel() < n + 1:
+            self.h_off = torch.empty(max(n + 1, 1 << 12), dtype=torch.int64, pin_memory=True)
+        if self.h_idx is None:
+            self.h_idx = torch.empty(1 << 16, dtype=torch.int32, pin_memory=True)
+        for _ in range(2):
+            try:
+                total, k_max, bad, done = _PACKER.pack_into(
+                    batched_indices, self.h_idx.data_ptr(), self.h_idx.numel(),
+                    self.h_off.data_ptr(), self.h_off.numel())
+            except (TypeError, OverflowError):
+                return None
+            if done:
+                if total == 0:
+                    self.h_idx[0] = 0
+                return self.h_idx[:max(total, 1)], self.h_off[:n + 1], k_max, bad
+            self.h_idx = torch.empty(max(total, 2 * self.h_idx.numel()), dtype=torch.int32,
+                                     pin_memory=True)
+        raise RuntimeError("batch packing did not fit its staging buffer")
+
+    def pack_arrays(self, arrays):
+        """The same for a list of int32 numpy arrays (numpy concatenation into
+        the pinned buffers); returns (h_idx, h_off, k_max)."""
+        n = len(arrays)
+        lengths = np.fromiter((a.size for a in arrays), dtype=np.int64, count=n)
+        total = int(lengths.sum())
+        if self._copied is not None:
+            self._copied.synchronize()
+        if self.h_off is None or self.h_off.numel() < n + 1:
+            self.h_off = torch.empty(max(n + 1, 1 << 12), dtype=torch.int64, pin_memory=True)
+        if self.h_idx is None or self.h_idx.numel() < max(total, 1):
+            self.h_idx = torch.empty(max(total, 1 << 16), dtype=torch.int32, pin_memory=True)
+        off = self.h_off[:n + 1].numpy()
+        off[0] = 0
+        np.cumsum(lengths, out=off[1:])
+        if total:
+            np.concatenate(arrays, out=self.h_idx[:total].numpy())
+        else:
+            self.h_idx[0] = 0
+        k_max = int(lengths.max()) if n else 0
+        return self.h_idx[:max(total, 1)], self.h_off[:n + 1], k_max
+
+    def mark(self, stream: torch.cuda.Stream) -> None:
+        if self._copied is None:
+            self._copied = torch.cuda.Event()
+        self._copied.record(stream)
+
+
 class DistanceRunner:
     """Device-level max_zeros: inputs and outputs are torch CUDA tensors.
 
@@ -247,39 +316,7 @@ class DistanceOracleCUDABP:
         self.device = self.runner.device
         self._stream = torch.cuda.Stream(device=self.device)
         self._lock = threading.Lock()
-        # Pinned staging of the packed batch, reused across calls; the event
-        # marks the end of the last call's host-to-device copies out of it.
-        self._h_idx: torch.Tensor | None = None
-        self._h_off: torch.Tensor | None = None
-        self._staged: torch.cuda.Event | None = None
-
-    def _stage(self, batched_indices):
-        """Packs the batch straight into the pinned staging buffers (the C
-        packer); None when the packer is missing or the items are not ints.
-        Returns (h_idx, h_off, k_max, bad) views of the staging buffers."""
-        if _PACKER is None or not hasattr(_PACKER, "pack_into"):
-            return None
-        n = len(batched_indices)
-        if self._staged is not None:
-            self._staged.synchronize()  # the last copies out of the buffers are done
-        if self._h_off is None or self._h_off.numel() < n + 1:
-            self._h_off = torch.empty(max(n + 1, 1 << 12), dtype=torch.int64, pin_memory=True)
-        if self._h_idx is None:
-            self._h_idx = torch.empty(1 << 16, dtype=torch.int32, pin_memory=True)
-        for _ in range(2):
-            try:
-                total, k_max, bad, done = _PACKER.pack_into(
-                    batched_indices, self._h_idx.data_ptr(), self._h_idx.numel(),
-                    self._h_off.data_ptr(), self._h_off.numel())
-            except (TypeError, OverflowError):
-                return None
-            if done:
-                if total == 0:
-                    self._h_idx[0] = 0
-                return self._h_idx[:max(total, 1)], self._h_off[:n + 1], k_max, bad
-            self._h_idx = torch.empty(max(total, 2 * self._h_idx.numel()), dtype=torch.int32,
-                                      pin_memory=True)
-        raise RuntimeError("batch packing did not fit its staging buffer")
+        self._stage = PinnedBatchStage()
 
     def _runner_for(self, k_max: int, sampled: bool) -> DistanceRunner:
         """Launch shape: the fixed config, else the autotuned one for k_max."""
@@ -322,7 +359,7 @@ class DistanceOracleCUDABP:
     def _evaluate(self, batched_indices, target_distance, sample_count, sample_seed) -> list[int]:
         n = len(batched_indices)
         with self._lock, torch.cuda.device(self.device):
-            staged = self._stage(batched_indices)
+            staged = self._stage.pack(batched_indices)
             if staged is None:
                 flat, offsets, k_max = pack_sets(batched_indices)
                 bad = bool(flat.size) and (int(flat.min()) < 0 or int(flat.max()) >= N_POINTS)
@@ -346,9 +383,7 @@ class DistanceOracleCUDABP:
             with torch.cuda.stream(s):
                 d_idx = h_idx.to(self.device, non_blocking=True)
                 d_off = h_off.to(self.device, non_blocking=True)
-                if self._staged is None:
-                    self._staged = torch.cuda.Event()
-                self._staged.record(s)
+                self._stage.mark(s)
                 d_td = None
                 if td_arr is not None:
                     d_td = torch.from_numpy(td_arr).pin_memory().to(self.device, non_blocking=True)

@@ -237,7 +237,7 @@ class ToricBatchServer:
 
     def __init__(self, device_id: int = 0, M: np.ndarray | None = None, *, k_max: int = 21,
                  max_batch: int = 1 << 16, dedup: bool = True, cache_size: int = 1 << 20):
-        from .distance import MAX_EXACT_K, DistanceRunner, LaunchConfig
+        from .distance import MAX_EXACT_K, DistanceRunner, LaunchConfig, PinnedBatchStage
 
         if not 0 <= k_max <= MAX_EXACT_K:
             raise ValueError("k_max must lie in 0..21")
@@ -249,6 +249,7 @@ class ToricBatchServer:
         self.cache_size = cache_size
         self._lib = _lib.load()
         self._runner = DistanceRunner(self.ctx, LaunchConfig())
+        self._stage = PinnedBatchStage()  # used by the worker thread only
         self._stream = torch.cuda.Stream(device=self.device)
         self._cache: dict[int, tuple[int, int]] = {}  # canonical mask -> (max_zeros, td)
         self._cv = threading.Condition()
@@ -349,16 +350,14 @@ class ToricBatchServer:
         return h.numpy().view(np.uint64).copy()
 
     def _run(self, sets: list[np.ndarray], tds: list[int]) -> tuple[list[int], float]:
-        from .distance import pack_sets
-
-        flat, offsets, k_max = pack_sets(sets)
         n = len(sets)
         s = self._stream
         runner = self._runner
+        h_idx, h_off, k_max = self._stage.pack_arrays(sets)
         with torch.cuda.device(self.device), torch.cuda.stream(s):
-            d_idx = torch.from_numpy(flat if flat.size else np.zeros(1, np.int32)).pin_memory()
-            d_idx = d_idx.to(self.device, non_blocking=True)
-            d_off = torch.from_numpy(offsets).pin_memory().to(self.device, non_blocking=True)
+            d_idx = h_idx.to(self.device, non_blocking=True)
+            d_off = h_off.to(self.device, non_blocking=True)
+            self._stage.mark(s)
             d_td = torch.from_numpy(np.asarray(tds, dtype=np.int32)).pin_memory().to(
                 self.device, non_blocking=True)
             d_out = torch.empty(n, dtype=torch.int32, device=self.device)
