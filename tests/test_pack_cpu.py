@@ -101,3 +101,48 @@ def test_pack_into_caller_buffers(packer):
     assert packer.pack_into([[1, 50]], f.ctypes.data, f.size, o.ctypes.data, o.size)[2]
     with pytest.raises(TypeError):
         packer.pack_into([[1, "a"]], f.ctypes.data, f.size, o.ctypes.data, o.size)
+
+
+@pytest.fixture
+def host_stage(packer, monkeypatch):
+    """PinnedBatchStage on a machine without a GPU: pinned allocation becomes
+    ordinary allocation (the buffers' contents and sizes are what is tested)."""
+    import torch
+
+    real_empty = torch.empty
+
+    def empty(*args, pin_memory=False, **kwargs):
+        return real_empty(*args, **kwargs)
+
+    monkeypatch.setattr(torch, "empty", empty)
+    monkeypatch.setattr(D, "_PACKER", packer)
+    return D.PinnedBatchStage()
+
+
+def test_stage_pack_grows_and_matches(host_stage):
+    rng = np.random.default_rng(10)
+    for n in (1, 100, 9000):  # the last one outgrows both initial buffers
+        batch = [rng.choice(49, size=int(rng.integers(0, 22)), replace=False).tolist()
+                 for _ in range(n)]
+        h_idx, h_off, k_max, bad = host_stage.pack(batch)
+        flat, offsets, k_ref = D.pack_sets(batch)
+        assert not bad and k_max == k_ref
+        np.testing.assert_array_equal(h_off.numpy(), offsets)
+        np.testing.assert_array_equal(h_idx.numpy()[:flat.size], flat)
+        assert h_idx.numel() == max(flat.size, 1)
+    assert host_stage.pack([[], []])[0].tolist() == [0]
+    assert host_stage.pack([[1.5, 2]]) is None  # non-int items: the caller packs with numpy
+    assert host_stage.pack([[7, 49]])[3]  # out of range flagged
+
+
+def test_stage_pack_arrays(host_stage):
+    rng = np.random.default_rng(11)
+    arrays = [np.sort(rng.choice(49, size=int(rng.integers(0, 16)), replace=False)).astype(np.int32)
+              for _ in range(5000)]
+    h_idx, h_off, k_max = host_stage.pack_arrays(arrays)
+    flat = np.concatenate(arrays)
+    np.testing.assert_array_equal(h_idx.numpy()[:flat.size], flat)
+    np.testing.assert_array_equal(h_off.numpy(), np.concatenate([[0], np.cumsum([a.size for a in arrays])]))
+    assert k_max == max(a.size for a in arrays)
+    h_idx, h_off, k_max = host_stage.pack_arrays([np.zeros(0, np.int32)])
+    assert h_idx.tolist() == [0] and h_off.tolist() == [0, 0] and k_max == 0
