@@ -1,43 +1,41 @@
 // Information-set enumeration of max_zeros (Brouwer-Zimmermann).  Included by
 // distance.cu, whose GF(8) tables, descriptors and helpers it shares.
 //
-// max_zeros = 49 - d, d the minimum weight of a nonzero codeword.  For a code
-// of k rows, a warp finds information sets I_1..I_s: pairwise disjoint sets of
-// columns, the first m of them of rank k ("full") and possibly a last one of
-// rank r = k - delta ("partial").  Gauss-Jordan elimination on I_j gives a
-// generator G_j of the same code that is the identity on I_j's pivot columns,
-// and rows r..k-1 of a partial set's G_j vanish on all of its columns.  A
-// codeword c = u G_j then has wt(c restricted to I_j) >= wt(u) - delta_j.
-// Level w enumerates, for every set, the projective messages u of weight
-// exactly w, so once levels 1..L are complete every codeword not yet seen
-// has weight >= m (L + 1) + max(0, L + 1 - delta) (the columns of different
-// sets are disjoint).  A code is finished when
-//   * its best weight is <= that bound (the best weight is then d), or
-//   * all k levels are complete (every message has been seen), or
-//   * a weight below the target distance appears (the decision of the early
-//     exit: max_zeros > 49 - target_distance).
+// max_zeros = 49 - d, d the minimum weight of a nonzero codeword.  Gauss-Jordan
+// elimination on an information set I (k columns of rank k) gives a generator
+// of the code that is the identity on I, so a codeword c = u G equals the
+// message u on I.  Level w enumerates the projective messages of weight
+// exactly w.  After levels 1..L every codeword not yet seen weighs at least
+//   * ceil(49 (L + 1) / k) for a toric code, from one set: the torus
+//     translations permute the 49 columns regularly and map the code onto
+//     itself, so every translate of I is an information set too, and each
+//     column lies in exactly k of the 49 translates;
+//   * m (L + 1) + max(0, L + 1 - delta) for any other matrix, from pairwise
+//     disjoint sets I_1..I_s found by greedy elimination over column orders
+//     (m full sets, and possibly a last one of rank k - delta).
+// A code is finished when its best weight is <= that bound (the best weight
+// is then d), when all k levels are complete, or when a weight below the
+// target distance appears (the early-exit decision).  One lane holds one row,
+// bit-sliced over the 49 columns, so a pivot step is a ballot, a row swap and
+// one broadcast; each set's columns are reordered with the pivots last (in
+// the high word).
 //
-// Sets are found by greedy elimination over a column order; the identity
-// order first, then up to kIsTries - 1 pseudo-random orders (a fixed
-// sequence), keeping the order with the most full sets and then the largest
-// partial rank.  One lane holds one row, bit-sliced over the 49 columns, so a
-// pivot step is a ballot, a row swap and one broadcast.
+// Levels 1 to 3 run as one warp-per-set launch (levels123_kernel).  From level
+// 4 on, each level is a launch triple: plan_level_kernel finishes the codes
+// whose bound is met and sizes the level for the others, scan_level_kernel
+// picks the task size and the offsets, and walk_level_kernel hands the tasks
+// to a persistent grid.  No code starts a level before the previous one is
+// complete, so no work is spent on levels a code turns out not to need.
 //
-// Walk.  A support T of w rows has its first row at coefficient 1; the other
-// w - 1 rows walk a reflected base-7 Gray code over alpha^0..alpha^6, one XOR
-// of a precomputed delta (alpha^v + alpha^(v+1)) g per codeword.  The two
-// fastest digits form straight-line blocks of 49 codewords with their deltas
-// in registers; a task is a range of blocks (of one or more supports), and
-// can start at any block because the Gray position of a block start has a
-// closed form.
-//
-// Levels run one launch at a time: plan_level_kernel finishes the codes whose
-// bound is met and sizes the next level of the others, scan_level_kernel
-// picks the task size from the level's total work (about eight tasks per
-// resident thread, at most ~16807 codewords) and the offsets, and
-// walk_level_kernel hands the tasks to a persistent grid.  No code starts a
-// level before the previous one is complete, so no work is spent on levels a
-// code turns out not to need.
+// Walk.  A support of w rows has its last row at coefficient 1.  A block is 49
+// codewords: digit 0 swept through its 7 multiples, digit 1 stepping
+// alpha^0..alpha^6 between the sweeps; digits 2.. follow a reflected base-7
+// Gray code over the blocks, whose start state has a closed form, so a task
+// (a range of blocks) may start anywhere.  The zeros of a sweep's 7 codewords
+// on the 32 low columns are one-LOP3 selections in the domain W = P / g; a
+// threshold test on them (single counts, or pairs of codewords at high
+// thresholds) sends the rare sweep that may hold a lighter codeword to an
+// exact count.
 #pragma once
 
 namespace tg {
