@@ -49,7 +49,7 @@ POPC_PER_CODEWORD_INFOSET = 8.0 / 7.0
 
 # --enumeration: (TG_ENUM_* value, description)
 ENUMERATIONS = {
-    "auto": (0, "auto: information sets for k >= 10, orbit (projective + torus "
+    "auto": (0, "auto: information sets for k >= 2, orbit (projective + torus "
                 "normalisation) below"),
     "projective": (1, "projective messages"),
     "orbit": (2, "orbit (projective + torus normalisation)"),
@@ -61,7 +61,7 @@ def launches_per_step(k_max: int, enumeration: str) -> int:
     """Kernels per step: prep_exact, scan_tasks and the enumeration walk; with
     information sets also prep_infoset, levels123 (levels 1 to 3), per level
     4..k_max plan, scan and walk, and finalize_infoset."""
-    infoset = enumeration == "infoset" or (enumeration == "auto" and k_max >= 10)
+    infoset = enumeration == "infoset" or (enumeration == "auto" and k_max >= 2)
     return 3 + ((3 + 3 * max(0, k_max - 3)) if infoset else 0)
 
 

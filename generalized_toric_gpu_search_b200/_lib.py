@@ -29,7 +29,7 @@ TG_ENUM_AUTO = 0
 TG_ENUM_PROJECTIVE = 1
 TG_ENUM_ORBIT = 2
 TG_ENUM_INFOSET = 3
-TG_INFOSET_AUTO_MIN_K = 10
+TG_INFOSET_AUTO_MIN_K = 2
 TG_WALK_ENUMERATION = 1
 TG_WALK_INFOSET = 2
 TG_VARIANT_AUTO = 0

@@ -223,7 +223,7 @@ class ToricBatchServer:
     """max_zeros requests served as continuous micro-batches of the batch path.
 
     A worker thread takes every request waiting when the GPU becomes free and
-    runs them as one tg_max_zeros batch (information sets for k >= 10, one
+    runs them as one tg_max_zeros batch (information sets for k >= 2, one
     launch per level, so a batch of any size costs about the same fixed
     launch overhead plus its work).  Requests that arrive meanwhile form the
     next batch.  Canonical dedup as in ToricServer: the AGL2(F7) canonical

@@ -85,8 +85,9 @@ int tg_context_is_toric(const tg_context* ctx, int32_t* h_is_toric);
 /* Exact enumeration strategies.  All give the same max_zeros (and the same
  * pass/fail decision under an early exit); they differ in how many codewords
  * they evaluate.
- *   AUTO        sets with k >= TG_INFOSET_AUTO_MIN_K by information sets, the
- *               others by orbit (toric context) or projective enumeration
+ *   AUTO        sets with k >= TG_INFOSET_AUTO_MIN_K (2) by information
+ *               sets, the others (k = 1) by orbit (toric context) or
+ *               projective enumeration
  *   PROJECTIVE  every message whose first nonzero coefficient is 1
  *   ORBIT       projective + torus-orbit normalisation (toric context only)
  *   INFOSET     information sets (Brouwer-Zimmermann) for every set, k >= 2:
@@ -99,7 +100,7 @@ enum {
   TG_ENUM_ORBIT = 2,
   TG_ENUM_INFOSET = 3
 };
-#define TG_INFOSET_AUTO_MIN_K 10
+#define TG_INFOSET_AUTO_MIN_K 2
 enum {
   TG_VARIANT_AUTO = 0,      /* histogram when the context is toric            */
   TG_VARIANT_HISTOGRAM = 1, /* last row via an 8-bin zero histogram           */

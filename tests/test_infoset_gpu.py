@@ -110,7 +110,7 @@ def test_large_k_threshold_decisions(infoset, orbit):
 
 
 def test_auto_mixes_both_paths(M, orbit):
-    """AUTO sends k >= 10 to information sets and the rest to the orbit walk,
+    """AUTO sends k >= 2 to information sets and k = 1 to the orbit walk,
     in one batch, with per-set thresholds."""
     from generalized_toric_gpu_search_b200 import _lib
 
