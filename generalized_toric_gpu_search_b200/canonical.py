@@ -18,7 +18,8 @@ import torch
 
 from . import _lib
 from .distance import ToricContext, _require_cuda
-from .tables import N_POINTS, build_eval_matrix, precompute_gl2_perms, rel_table
+from .tables import N_POINTS, build_eval_matrix, precompute_gl2_perms
+from .tables import rel_table as _difference_table
 
 MAX_KEY_K = 16
 
@@ -26,17 +27,21 @@ MAX_KEY_K = 16
 class CanonicalOracle:
     """GPU canonical-form engine; one instance per CUDA device.
 
+    The signature is the reference's, `CanonicalOracle(device_id, gl2_perms,
+    rel_table)` (kernel_canon.py:137-142), positionally or by keyword.
     `gl2_perms` and `rel_table` are accepted for interface compatibility and
-    checked against the tables the library builds itself."""
+    checked against the tables the library builds itself.  `rel_table_arr`
+    is an older keyword-only spelling of `rel_table`."""
 
     def __init__(self, device_id: int, gl2_perms: np.ndarray | None = None,
+                 rel_table: np.ndarray | None = None, *,
                  rel_table_arr: np.ndarray | None = None):
         _require_cuda(device_id)
+        rel = _pick_rel_table(rel_table, rel_table_arr)
         if gl2_perms is not None and not np.array_equal(np.asarray(gl2_perms),
                                                         precompute_gl2_perms()):
             raise ValueError("gl2_perms differs from GL2(F7) on the 49 exponent points")
-        if rel_table_arr is not None and not np.array_equal(np.asarray(rel_table_arr),
-                                                            rel_table()):
+        if rel is not None and not np.array_equal(np.asarray(rel), _difference_table()):
             raise ValueError("rel_table differs from the Z_7^2 difference table")
         self.device_id = device_id
         self.ctx = ToricContext(device_id, build_eval_matrix())
@@ -135,12 +140,22 @@ class CanonicalOracle:
         return h.numpy().view(np.uint64).copy()
 
 
+def _pick_rel_table(rel_table, rel_table_arr):
+    if rel_table is not None and rel_table_arr is not None:
+        raise TypeError("pass rel_table or rel_table_arr, not both")
+    return rel_table if rel_table is not None else rel_table_arr
+
+
 def init_canon_oracle(device_id: int, gl2_perms: np.ndarray | None = None,
+                      rel_table: np.ndarray | None = None, *,
                       rel_table_arr: np.ndarray | None = None) -> CanonicalOracle:
-    """Builds a CanonicalOracle (kernel_canon.py:179-191)."""
+    """Builds a CanonicalOracle (kernel_canon.py:179-191).  The reference's
+    driver calls it as init_canon_oracle(device_id=..., gl2_perms=...,
+    rel_table=...) (champion_search_canonical.py:447-451)."""
+    rel = _pick_rel_table(rel_table, rel_table_arr)
     _, _, _, name = _lib.device_info(device_id)
     print(f"[canon] GPU {device_id}: {name} — canonical kernel ready")
-    return CanonicalOracle(device_id, gl2_perms, rel_table_arr)
+    return CanonicalOracle(device_id, gl2_perms, rel)
 
 
 class CanonicalDedup:

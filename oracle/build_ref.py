@@ -12,13 +12,19 @@ oracle/ref_harness.cu into oracle/_ref/libref_kernels.so.  oracle/_ref/ is
 git-ignored (nothing of the reference is committed); a copy of the working tree
 taken to a machine without the reference checkout carries the built library.
 
-Usage: python oracle/build_ref.py [--reference /root/reference]
+The reference checkout is taken from --reference, else from the
+TG_REFERENCE_DIR environment variable, else from the recipe's fallback
+location below (where the build container mounts it); build() does nothing
+when none of them holds the reference.
+
+Usage: python oracle/build_ref.py [--reference DIR]
 """
 
 from __future__ import annotations
 
 import argparse
 import importlib
+import os
 import shutil
 import subprocess
 import sys
@@ -28,7 +34,13 @@ from pathlib import Path
 ORACLE_DIR = Path(__file__).resolve().parent
 OUT_DIR = ORACLE_DIR / "_ref"
 LIB = OUT_DIR / "libref_kernels.so"
-DEFAULT_REFERENCE = Path("/root/reference")
+FALLBACK_REFERENCE = Path("/root/reference")
+
+
+def reference_dir() -> Path:
+    """$TG_REFERENCE_DIR when set, else the fallback location."""
+    env = os.environ.get("TG_REFERENCE_DIR")
+    return Path(env) if env else FALLBACK_REFERENCE
 
 
 class _Stub(types.ModuleType):
@@ -55,9 +67,10 @@ def extract_sources(reference: Path) -> dict[str, str]:
                 sys.modules[k] = v
 
 
-def build(reference: Path = DEFAULT_REFERENCE, force: bool = False) -> Path | None:
+def build(reference: Path | None = None, force: bool = False) -> Path | None:
     """Builds oracle/_ref/libref_kernels.so; returns None when the reference
     checkout is absent (a machine without it uses the prebuilt library)."""
+    reference = Path(reference) if reference is not None else reference_dir()
     if not (reference / "kernel_cuda_bp.py").exists():
         return LIB if LIB.exists() else None
     harness = ORACLE_DIR / "ref_harness.cu"
@@ -82,7 +95,8 @@ def build(reference: Path = DEFAULT_REFERENCE, force: bool = False) -> Path | No
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", type=Path, default=DEFAULT_REFERENCE)
+    ap.add_argument("--reference", type=Path, default=None,
+                    help="reference checkout (default: $TG_REFERENCE_DIR, else the fallback)")
     ap.add_argument("--force", action="store_true")
     args = ap.parse_args()
     print(build(args.reference, args.force))

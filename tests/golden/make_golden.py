@@ -1,7 +1,7 @@
 """Generates tests/golden/golden.json from the reference's own Python code.
 
-Run in a checkout that has the reference at /root/reference (or pass
---reference).  The reference modules import pyopencl/cupy at module level, so
+Run with the reference checkout given by --reference or the
+TG_REFERENCE_DIR environment variable (one of them is required).  The reference modules import pyopencl/cupy at module level, so
 both are stubbed; the functions used here are pure numpy/Python:
   gf8.MUL_TABLE                                 (gf8.py:24-38)
   precompute.build_eval_matrix                  (precompute.py:32-43)
@@ -18,6 +18,7 @@ from __future__ import annotations
 import argparse
 import hashlib
 import json
+import os
 import random
 import sys
 import types
@@ -49,8 +50,11 @@ def brute_max_zeros(S, M, mul):
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("TG_REFERENCE_DIR"),
+                    help="reference checkout (default: $TG_REFERENCE_DIR)")
     args = ap.parse_args()
+    if not args.reference:
+        ap.error("give --reference or set TG_REFERENCE_DIR")
     sys.modules["pyopencl"] = _Stub("pyopencl")
     sys.modules["cupy"] = _Stub("cupy")
     sys.path.insert(0, args.reference)
