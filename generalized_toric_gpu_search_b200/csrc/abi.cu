@@ -364,6 +364,105 @@ int tg_max_zeros(tg_context* ctx, const tg_distance_params* p, const int32_t* d_
   return run_walk(a, ctx->sm_count, bps, tpb, s);
 }
 
+}  // extern "C"
+
+namespace tg {
+
+// Workspace of tg_max_zeros_witness: the first pass (the caller's
+// parameters), the witness pass (information sets for every k >= 1), and the
+// pass's values, targets, claim words and pivot columns.
+struct WitLayout {
+  WsLayout p1, p2;
+  size_t off2, out2, td2, lock, piv, total;
+};
+
+static tg_distance_params witness_pass_params(const tg_distance_params& p) {
+  tg_distance_params q = p;
+  q.enumeration = kEnumInfosetAll;
+  q.target_distance = 1;
+  q.sample_count = 0;
+  return q;
+}
+
+static WitLayout witness_layout(const tg_distance_params& p) {
+  WitLayout L{};
+  const size_t n = size_t(p.n_sets > 0 ? p.n_sets : 0);
+  L.p1 = ws_layout(p);
+  L.p2 = ws_layout(witness_pass_params(p));
+  size_t off = align_ws(L.p1.total);
+  L.off2 = off;  off = align_ws(off + L.p2.total);
+  L.out2 = off;  off = align_ws(off + n * sizeof(int32_t));
+  L.td2 = off;   off = align_ws(off + n * sizeof(int32_t));
+  L.lock = off;  off = align_ws(off + n * sizeof(int32_t));
+  L.piv = off;   off = align_ws(off + n * kIsMaxSets * sizeof(uint64_t));
+  L.total = off;
+  return L;
+}
+
+}  // namespace tg
+
+extern "C" {
+
+int tg_witness_workspace_size(const tg_distance_params* p, size_t* h_bytes) {
+  int st = check_distance_params(p);
+  if (st) return st;
+  if (!h_bytes) return invalid("NULL h_bytes");
+  if (p->sample_count > 0) return invalid("witnesses are defined for exact max_zeros only");
+  *h_bytes = witness_layout(*p).total;
+  return TG_OK;
+}
+
+int tg_max_zeros_witness(tg_context* ctx, const tg_distance_params* p, const int32_t* d_indices,
+                         const int64_t* d_offsets, const int32_t* d_target,
+                         const int32_t* d_set_ids, int32_t* d_out, uint8_t* d_witness,
+                         void* d_workspace, size_t workspace_bytes, void* stream) {
+  if (!ctx) return invalid("tg_max_zeros_witness: NULL context");
+  int st = check_distance_params(p);
+  if (st) return st;
+  if (p->sample_count > 0) return invalid("witnesses are defined for exact max_zeros only");
+  if (p->n_sets == 0) return TG_OK;
+  if (!d_witness) return invalid("tg_max_zeros_witness: NULL witness buffer");
+  const WitLayout W = witness_layout(*p);
+  if (workspace_bytes < W.total) {
+    set_last_error("tg_max_zeros_witness: workspace has %zu bytes, needs %zu", workspace_bytes,
+                   W.total);
+    return TG_ERR_WORKSPACE;
+  }
+  DistArgs a1;
+  st = bind_distance(ctx, p, d_indices, d_offsets, d_target, d_set_ids, d_out, d_workspace,
+                     workspace_bytes, true, a1);
+  if (st) return st;
+  DeviceGuard g(ctx->device);
+  if (g.error() != cudaSuccess) return cuda_fail(g.error(), "cudaSetDevice");
+  const cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int bps, tpb;
+  launch_shape(p, &bps, &tpb);
+  // Pass 1: max_zeros as tg_max_zeros computes it.
+  st = run_prepare(a1, s);
+  if (!st) st = run_walk(a1, ctx->sm_count, bps, tpb, s);
+  if (st) return st;
+  // Pass 2: information sets with per-set targets 50 - out, recording the
+  // first codeword below each target.
+  uint8_t* b = static_cast<uint8_t*>(d_workspace);
+  DistArgs a2 = a1;
+  bind_workspace(a2, W.p2, b + W.off2);
+  a2.sample_count = 0;
+  a2.td_default = 1;
+  a2.target = reinterpret_cast<int32_t*>(b + W.td2);
+  a2.out = reinterpret_cast<int32_t*>(b + W.out2);
+  a2.is_piv = reinterpret_cast<uint64_t*>(b + W.piv);
+  a2.witness = d_witness;
+  a2.wit_lock = reinterpret_cast<int32_t*>(b + W.lock);
+  cudaError_t e = cudaMemsetAsync(d_witness, 0, size_t(p->n_sets) * kN, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(a2.wit_lock, 0, size_t(p->n_sets) * sizeof(int32_t), s);
+  if (e != cudaSuccess) return cuda_fail(e, "tg_max_zeros_witness: clear witness buffers");
+  st = run_witness_targets(d_out, d_offsets, reinterpret_cast<int32_t*>(b + W.td2), p->n_sets, s);
+  if (!st) st = run_prepare(a2, s);
+  if (!st) st = run_walk(a2, ctx->sm_count, bps, tpb, s);
+  if (!st) st = run_witness_finish(a2, d_out, a1.hdr, s);
+  return st;
+}
+
 int tg_distance_status(const tg_distance_params* p, const void* d_workspace, void* stream,
                        int32_t* h_status) {
   int st = check_distance_params(p);

@@ -85,6 +85,7 @@ int upload_field_tables(int device) {
 // ---------------------------------------------------------------------------
 
 static size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+size_t align_ws(size_t x) { return align256(x); }
 
 int max_patterns(int H) {
   if (H <= 0) return 1;
@@ -100,6 +101,7 @@ constexpr int kNever = 1 << 20;
 int infoset_min_k(const tg_distance_params& p) {
   if (p.sample_count > 0) return kNever;
   if (p.enumeration == TG_ENUM_INFOSET) return 2;
+  if (p.enumeration == kEnumInfosetAll) return 1;
   if (p.enumeration == TG_ENUM_AUTO) return TG_INFOSET_AUTO_MIN_K;
   return kNever;
 }
@@ -901,13 +903,33 @@ int run_walk(const DistArgs& args, int sm_count, int blocks_per_sm, int tpb, cud
     for (int w = 4; w <= args.k_max; ++w) {
       plan_level_kernel<<<plan_grid, 256, 0, s>>>(la, w);
       scan_level_kernel<<<1, kScanThreads, 0, s>>>(la, w);
-      walk_level_kernel<kIsWalkThreads, kPerSm><<<sm_count * kPerSm, kIsWalkThreads, 0, s>>>(la, w);
+      if (la.witness)
+        walk_level_kernel<kIsWalkThreads, kPerSm, true>
+            <<<sm_count * kPerSm, kIsWalkThreads, 0, s>>>(la, w);
+      else
+        walk_level_kernel<kIsWalkThreads, kPerSm, false>
+            <<<sm_count * kPerSm, kIsWalkThreads, 0, s>>>(la, w);
     }
     finalize_infoset_kernel<<<plan_grid, 256, 0, s>>>(la);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "information-set walk launch");
   }
   return TG_OK;
+}
+
+int run_witness_targets(const int32_t* out, const int64_t* off, int32_t* td, int n,
+                        cudaStream_t s) {
+  if (n <= 0) return TG_OK;
+  witness_targets_kernel<<<(n + 255) / 256, 256, 0, s>>>(out, off, td, n);
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? TG_OK : cuda_fail(e, "witness target launch");
+}
+
+int run_witness_finish(const DistArgs& a2, int32_t* out, WsHeader* hdr1, cudaStream_t s) {
+  if (a2.n <= 0) return TG_OK;
+  witness_finish_kernel<<<(a2.n + 255) / 256, 256, 0, s>>>(a2, out, hdr1);
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? TG_OK : cuda_fail(e, "witness finish launch");
 }
 
 }  // namespace tg

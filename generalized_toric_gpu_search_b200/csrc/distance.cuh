@@ -101,8 +101,18 @@ struct DistArgs {
   uint64_t* is_units;            // units of the current level per code
   uint64_t* is_off;              // task offsets of the current level (n + 1)
   int32_t* is_best;              // smallest weight met per code
+  // Witness pass only (NULL otherwise): per code and set the pivot columns
+  // (kIsMaxSets words), the witness codewords (49 GF(8) symbols per code, in
+  // the original column order) and one claim word per code.
+  uint64_t* is_piv;
+  uint8_t* witness;
+  int32_t* wit_lock;
   DeviceTables tab;
 };
+
+// Internal enumeration of the witness pass: information sets for every
+// k >= 1 (not a TG_ENUM_* value of the C ABI).
+constexpr int kEnumInfosetAll = 16;
 
 int upload_field_tables(int device);
 int max_patterns(int H);
@@ -116,5 +126,13 @@ constexpr int kWalkEnumeration = 1;
 constexpr int kWalkInfoset = 2;
 int run_walk(const DistArgs& args, int sm_count, int blocks_per_sm, int tpb, cudaStream_t s,
              int parts = kWalkEnumeration | kWalkInfoset);
+// Witness pass helpers: per-code targets 50 - out (the walk then stops at the
+// first codeword with out zeros or more), and the copy of the pass's values
+// into out with a check that every evaluated code got its witness (status
+// into hdr1).
+int run_witness_targets(const int32_t* out, const int64_t* off, int32_t* td, int n,
+                        cudaStream_t s);
+int run_witness_finish(const DistArgs& a2, int32_t* out, WsHeader* hdr1, cudaStream_t s);
+size_t align_ws(size_t x);
 
 }  // namespace tg

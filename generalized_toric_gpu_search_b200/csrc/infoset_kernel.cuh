@@ -224,6 +224,7 @@ __global__ void __launch_bounds__(kIsPrepWarps * 32) prep_infoset_kernel(DistArg
     } else {
       is_reorder_columns(used, p0, p1, p2);
       is_store_set(base, lane, k, p0, p1, p2);
+      if (a.is_piv && lane == 0) a.is_piv[size_t(c) * kIsMaxSets] = used;
       n_sets = 1;
       m_full = 1;
       flags |= kTorusBoundFlag;
@@ -271,6 +272,7 @@ __global__ void __launch_bounds__(kIsPrepWarps * 32) prep_infoset_kernel(DistArg
         uint64_t q0 = p0, q1 = p1, q2 = p2;
         is_reorder_columns(used & ~used_before, q0, q1, q2);
         is_store_set(base + size_t(n_sets) * k * kIsVecPerRow, lane, k, q0, q1, q2);
+        if (a.is_piv && lane == 0) a.is_piv[size_t(c) * kIsMaxSets + n_sets] = used & ~used_before;
         ++n_sets;
         if (r < k) {
           delta = k - r;
@@ -500,6 +502,60 @@ __device__ __forceinline__ const V6* is_block_move(const V6* rows, const uint16_
   return rows + dig[tz * kStride] + 1 + v;
 }
 
+// Where the witness pass records a codeword of one code: the pivot columns of
+// the information set it was found on, the code's 49-symbol output row and
+// its claim word (first writer wins).
+struct WitOut {
+  const uint64_t* piv;
+  uint8_t* dst;
+  int32_t* lock;
+};
+
+__device__ __forceinline__ WitOut wit_out(const DistArgs& a, int c, int j) {
+  return WitOut{a.is_piv + size_t(c) * kIsMaxSets + j, a.witness + size_t(c) * kN,
+                a.wit_lock + c};
+}
+
+// Records a codeword, given in its information set's column order (positions
+// 0..31 in the lo words, 32..48 in bits 0..16 of the hi words), as the code's
+// witness in the original column order: the set's non-pivot columns first
+// (increasing), then its pivots, as prep_infoset_kernel ordered them.  Only
+// the first caller per code writes, so the row is never torn.
+__device__ __noinline__ void is_put_witness(WitOut wo, uint32_t l0, uint32_t l1, uint32_t l2,
+                                            uint32_t h0, uint32_t h1, uint32_t h2) {
+  if (atomicCAS(wo.lock, 0, 1) != 0) return;
+  const uint64_t piv = *wo.piv & kMask49;
+  const uint64_t q0 = uint64_t(l0) | (uint64_t(h0 & kHiMask) << 32);
+  const uint64_t q1 = uint64_t(l1) | (uint64_t(h1 & kHiMask) << 32);
+  const uint64_t q2 = uint64_t(l2) | (uint64_t(h2 & kHiMask) << 32);
+  uint64_t rest = ~piv & kMask49, tail = piv;
+  for (int d = 0; d < kN; ++d) {
+    const bool front = rest != 0ull;
+    const uint64_t pick = front ? rest : tail;
+    const int col = __ffsll(static_cast<long long>(pick)) - 1;
+    if (front) rest &= rest - 1ull;
+    else tail &= tail - 1ull;
+    wo.dst[col] = uint8_t(((q0 >> d) & 1ull) | (((q1 >> d) & 1ull) << 1) |
+                          (((q2 >> d) & 1ull) << 2));
+  }
+}
+
+// is_sweep_exact of the witness pass: also records the first codeword
+// lighter than wthr.
+__device__ __noinline__ int is_sweep_exact_w(V6 P, const V6* g_row, int wmin, WitOut wo,
+                                             int wthr) {
+  V6 g = v6_ldg(g_row);
+  for (int v = 0; v < 7; ++v) {
+    const uint32_t x0 = P.l0 ^ g.l0, x1 = P.l1 ^ g.l1, x2 = P.l2 ^ g.l2;
+    const uint32_t y0 = P.h0 ^ g.h0, y1 = P.h1 ^ g.h1, y2 = P.h2 ^ g.h2;
+    const int wt = __popc(lop3<0xFE>(x0, x1, x2)) + __popc(lop3<0xFE>(y0, y1, y2));
+    if (wt < wthr) is_put_witness(wo, x0, x1, x2, y0, y1, y2);
+    wmin = min(wmin, wt);
+    v6_alpha_pow(g, 1);
+  }
+  return wmin;
+}
+
 // Exact weights of the seven codewords P + alpha^v g, v = 0..6, min'd into
 // wmin.
 __device__ __noinline__ int is_sweep_exact(V6 P, const V6* g_row, int wmin) {
@@ -574,9 +630,28 @@ __device__ __forceinline__ void gf8_scale32(uint32_t c, uint32_t& x0, uint32_t& 
 // sweep's zero counts z[v] (plus zz, the zeros on g's zero columns); the high
 // half is rebuilt from Ph, P's high word without digit 1's term, plus kC r1
 // (kC = digit 1's coefficient in this sweep).
+// Witness pass: rebuilds the codeword P + alpha^v g of a sweep from its W
+// domain state and records it.  The low columns of P are W g where g is
+// nonzero and Pz where g is zero; its high word is ph (digit 1's term
+// included); gh is the high word of alpha^v g.
+__device__ __noinline__ void is_sweep_witness(Pl3 W, Pl3 Pz, const V6* g_row, int v,
+                                              uint32_t ph0, uint32_t ph1, uint32_t ph2,
+                                              uint32_t gh0, uint32_t gh1, uint32_t gh2,
+                                              WitOut wo) {
+  Pl3 gl = pl3_lo(v6_ldg(g_row));
+  Pl3 P = pl3_mul(W, gl);
+  P.x0 |= Pz.x0;
+  P.x1 |= Pz.x1;
+  P.x2 |= Pz.x2;
+  for (int i = 0; i < v; ++i) gl = Pl3{gl.x2, gl.x0 ^ gl.x2, gl.x1};  // alpha gl
+  is_put_witness(wo, P.x0 ^ gl.x0, P.x1 ^ gl.x1, P.x2 ^ gl.x2, ph0 ^ gh0, ph1 ^ gh1, ph2 ^ gh2);
+}
+
+template <bool kW>
 __device__ __forceinline__ int is_sweep_fix(uint32_t kC, const int (&z)[7], int zz, uint32_t ph0,
                                             uint32_t ph1, uint32_t ph2, const V6* g_row,
-                                            const V6* r1_row, int wmin) {
+                                            const V6* r1_row, int wmin, const Pl3& W,
+                                            const Pl3& Pz, WitOut wo, int wthr) {
   uint32_t d0 = __ldg(&r1_row->h0), d1 = __ldg(&r1_row->h1), d2 = __ldg(&r1_row->h2);
   gf8_scale32(kC, d0, d1, d2);
   ph0 ^= d0;
@@ -587,7 +662,9 @@ __device__ __forceinline__ int is_sweep_fix(uint32_t kC, const int (&z)[7], int 
 #pragma unroll
   for (int v = 0; v < 7; ++v) {
     const int hi = __popc(lop3<0xFE>(ph0 ^ g0, ph1 ^ g1, ph2 ^ g2));
-    wmin = min(wmin, lo_base - z[v] + hi);
+    const int wt = lo_base - z[v] + hi;
+    if (kW && wt < wthr) is_sweep_witness(W, Pz, g_row, v, ph0, ph1, ph2, g0, g1, g2, wo);
+    wmin = min(wmin, wt);
     const uint32_t t = g2;  // g <- alpha g
     g2 = g1;
     g1 = g0 ^ t;
@@ -624,7 +701,8 @@ __device__ __forceinline__ int is_sweep_fix(uint32_t kC, const int (&z)[7], int 
     const int zm_ = __vimax3_s32(__vimax3_s32(z_[0], z_[1], z_[2]),                              \
                                  __vimax3_s32(z_[3], z_[4], z_[5]), z_[6]) - pz_;                \
     if (__builtin_expect(zm_ > thz, 0)) {                                                        \
-      wmin = is_sweep_fix(kC, z_, ngz - pz_, qh0, qh1, qh2, rows + r0, rows + r1, wmin);         \
+      wmin = is_sweep_fix<kW>(kC, z_, ngz - pz_, qh0, qh1, qh2, rows + r0, rows + r1, wmin, W,   \
+                              Pz, wo, wthr);                                                     \
       thz = thz_base - wmin;                                                                     \
     }                                                                                            \
   }
@@ -658,16 +736,17 @@ __device__ __forceinline__ int is_sweep_fix(uint32_t kC, const int (&z)[7], int 
 // W and Pz are the state of sweep 6; stepping back through digit 1's moves
 // (ez, stride kStride) gives each earlier sweep's.  Sweep s has digit 1 at
 // alpha^s (alpha^0..6 = 1, 2, 4, 3, 6, 7, 5, packed in nibbles).
-template <int kStride>
+template <int kStride, bool kW>
 __device__ __forceinline__ int is_block_fix(unsigned fl, Pl3 W, Pl3 Pz, const uint32_t* ez, int ngz,
                                          uint32_t qh0, uint32_t qh1, uint32_t qh2,
-                                         const V6* g_row, const V6* r1_row, int wmin) {
+                                         const V6* g_row, const V6* r1_row, int wmin, WitOut wo,
+                                         int wthr) {
   for (int s = 6; s >= 0 && fl != 0u; --s) {
     if ((fl >> s) & 1u) {
       TG_IS_ZCOUNTS(z_)
       const int pz_ = __popc(lop3<0xFE>(Pz.x0, Pz.x1, Pz.x2));
-      wmin = is_sweep_fix((0x05763421u >> (4 * s)) & 0xFu, z_, ngz - pz_, qh0, qh1, qh2, g_row,
-                          r1_row, wmin);
+      wmin = is_sweep_fix<kW>((0x05763421u >> (4 * s)) & 0xFu, z_, ngz - pz_, qh0, qh1, qh2,
+                              g_row, r1_row, wmin, W, Pz, wo, wthr);
       fl &= ~(1u << s);
     }
     if (s > 0) {
@@ -700,11 +779,11 @@ constexpr int kIsPairThr = 15;
 // P's high word without digit 1's term (qh, which only the block moves
 // change) is kept for the exact count of a rare sweep.  Returns the codewords
 // evaluated.
-template <int kStride>
+template <int kStride, bool kW>
 __device__ __forceinline__ unsigned long long is_walk_blocks(
     const V6& P, const V6* rows, uint32_t r0, uint32_t r1, const uint16_t* dig, uint32_t* ez,
     unsigned long long b0, unsigned long long nblk, int hb, int wthr, const int32_t* stop,
-    int& wmin) {
+    int& wmin, WitOut wo) {
   const Pl3 g = pl3_lo(v6_ldg(rows + r0));
   const Pl3 h = pl3_inv(g);
   const uint32_t gz = ~(g.x0 | g.x1 | g.x2);  // low columns where g is 0
@@ -788,7 +867,8 @@ __device__ __forceinline__ unsigned long long is_walk_blocks(
       TG_IS_SWEEP1(5, 7u); TG_IS_MOVE(5); TG_IS_SWEEP1(6, 5u);
     }
     if (__builtin_expect(fl != 0u, 0)) {
-      wmin = is_block_fix<kStride>(fl, W, Pz, ez, ngz, qh0, qh1, qh2, rows + r0, rows + r1, wmin);
+      wmin = is_block_fix<kStride, kW>(fl, W, Pz, ez, ngz, qh0, qh1, qh2, rows + r0, rows + r1,
+                                       wmin, wo, wthr);
       thz = thz_base - wmin;
     }
     if (wmin < wthr) break;
@@ -808,7 +888,7 @@ __device__ __forceinline__ unsigned long long is_walk_blocks(
 // smallest weight met (or wmin when none is smaller), and the codewords
 // evaluated in ncw.  dig and ez (stride kStride) are this thread's shared
 // scratch: the rows of digits 2..w-2 and digit 1's moves.
-template <int kStride>
+template <int kStride, bool kW>
 __device__ __forceinline__ int is_walk_units(const DistArgs& a,
                                              const unsigned long long (*bn)[kIsBinom],
                                              uint16_t* dig, uint32_t* ez, int c, int k, int w,
@@ -884,7 +964,9 @@ __device__ __forceinline__ int is_walk_units(const DistArgs& a,
       // that do not fit in the 17 high columns (k > 17).
       const int dj = int(j) == n_sets - 1 ? delta : 0;
       const int hb = max(0, w - dj - max(0, (k - dj) - 17));
-      ncw += is_walk_blocks<kStride>(P, rows, r0, r1, dig, ez, b, nblk, hb, wthr, stop, wmin);
+      const WitOut wo = kW ? wit_out(a, c, int(j)) : WitOut{nullptr, nullptr, nullptr};
+      ncw += is_walk_blocks<kStride, kW>(P, rows, r0, r1, dig, ez, b, nblk, hb, wthr, stop, wmin,
+                                         wo);
     }
     u += nblk;
     if (wmin < wthr) break;
@@ -894,7 +976,9 @@ __device__ __forceinline__ int is_walk_units(const DistArgs& a,
 
 constexpr int kIsMaxDigits = kMaxExactK - 3;  // digits 2..w-2, w <= 21
 
-template <int kTPB, int kMinBlocks>
+// kW: the witness pass (per-code targets 50 - max_zeros; the first codeword
+// below a target is recorded as that code's witness).
+template <int kTPB, int kMinBlocks, bool kW>
 __global__ void __launch_bounds__(kTPB, kMinBlocks) walk_level_kernel(DistArgs a, int w) {
   __shared__ unsigned long long s_binom[kIsBinom][kIsBinom];
   __shared__ uint16_t s_dig[kIsMaxDigits][kTPB];
@@ -944,8 +1028,8 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) walk_level_kernel(DistArgs a
         unsigned long long ncw = 0ull;
         // Codewords no lighter than the code's best so far cannot change it,
         // so the walk starts from that best.
-        wmin = is_walk_units<kTPB>(a, s_binom, my_dig, my_ez, c, a.desc[c].k, w, u0, u1,
-                                   kN - a.desc[c].tmax, best0, ncw);
+        wmin = is_walk_units<kTPB, kW>(a, s_binom, my_dig, my_ez, c, a.desc[c].k, w, u0, u1,
+                                       kN - a.desc[c].tmax, best0, ncw);
         evaluated += ncw;
       }
     }
@@ -993,13 +1077,18 @@ __global__ void __launch_bounds__(128) levels123_kernel(DistArgs a) {
   const int total = d.H * per_set;
   const V6* base = a.is_rows + size_t(c) * a.is_stride;
   int wmin = kN + 1;
+  // The witness pass records the first codeword lighter than wthr.
+  const bool wit = a.witness != nullptr;
+  const int wthr = kN - d.tmax;
   for (int u = lane; u < total; u += 32) {
     const int j = u / per_set;
     int r = u - j * per_set;
     const V6* rows = base + size_t(j) * k * kIsVecPerRow;
     if (r < n1) {
       const V6 P = v6_ldg(rows + r * kIsVecPerRow);
-      wmin = min(wmin, __popc(lop3<0xFE>(P.l0, P.l1, P.l2)) + __popc(lop3<0xFE>(P.h0, P.h1, P.h2)));
+      const int wt = __popc(lop3<0xFE>(P.l0, P.l1, P.l2)) + __popc(lop3<0xFE>(P.h0, P.h1, P.h2));
+      if (wit && wt < wthr) is_put_witness(wit_out(a, c, j), P.l0, P.l1, P.l2, P.h0, P.h1, P.h2);
+      wmin = min(wmin, wt);
       continue;
     }
     r -= n1;
@@ -1015,13 +1104,15 @@ __global__ void __launch_bounds__(128) levels123_kernel(DistArgs a) {
     const int q = r - p * (p - 1) / 2;
     const V6 Q = v6_ldg(rows + q * kIsVecPerRow);
     if (t < 0) {
-      wmin = is_sweep_exact(Q, rows + p * kIsVecPerRow, wmin);
+      wmin = wit ? is_sweep_exact_w(Q, rows + p * kIsVecPerRow, wmin, wit_out(a, c, j), wthr)
+                 : is_sweep_exact(Q, rows + p * kIsVecPerRow, wmin);
     } else {
       V6 X = v6_ldg(rows + p * kIsVecPerRow);  // alpha^s row_p, s = 0..6
       for (int s7 = 0; s7 < 7; ++s7) {
         V6 P = Q;
         v6_xor(P, X);
-        wmin = is_sweep_exact(P, rows + t * kIsVecPerRow, wmin);
+        wmin = wit ? is_sweep_exact_w(P, rows + t * kIsVecPerRow, wmin, wit_out(a, c, j), wthr)
+                   : is_sweep_exact(P, rows + t * kIsVecPerRow, wmin);
         v6_alpha_pow(X, 1);
       }
     }
@@ -1041,6 +1132,29 @@ __global__ void finalize_infoset_kernel(DistArgs a) {
   const CodeDesc d = a.desc[c];
   if ((d.flags & kIsCodeFlag) == 0 || (d.flags & kDecidedFlag) != 0) return;
   a.out[c] = kN - a.is_best[c];
+}
+
+// Targets of the witness pass: 50 - out, so that the pass stops at the first
+// codeword with at least out zeros (1 for an empty set).
+__global__ void witness_targets_kernel(const int32_t* out, const int64_t* off, int32_t* td, int n) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  const int m = min(max(out[c], 0), kN);
+  td[c] = off[c + 1] > off[c] ? kN + 1 - m : 1;
+}
+
+// After the witness pass: its values (the zeros of the recorded witnesses)
+// become the results; a code evaluated by the walk without a witness raises
+// TG_ERR_STATE, and any status of the pass is copied into the first pass's
+// header hdr1 (the one tg_distance_status reads).
+__global__ void witness_finish_kernel(DistArgs a2, int32_t* out, WsHeader* hdr1) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a2.n) return;
+  const CodeDesc d = a2.desc[c];
+  if ((d.flags & kIsCodeFlag) != 0 && (d.flags & kDecidedFlag) == 0 && a2.wit_lock[c] == 0)
+    report_status(hdr1, TG_ERR_STATE);
+  if (c == 0 && a2.hdr->status != TG_OK) report_status(hdr1, a2.hdr->status);
+  out[c] = a2.out[c];
 }
 
 }  // namespace tg

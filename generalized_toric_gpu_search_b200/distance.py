@@ -263,6 +263,30 @@ class DistanceRunner:
             "tg_max_zeros_walk_part",
         )
 
+    def run_witness(self, p: _lib.DistanceParams, d_indices: torch.Tensor,
+                    d_offsets: torch.Tensor, d_out: torch.Tensor, d_witness: torch.Tensor,
+                    d_target: torch.Tensor | None = None,
+                    stream: torch.cuda.Stream | None = None) -> None:
+        """Enqueues tg_max_zeros_witness: max_zeros into d_out and, per set, a
+        codeword with exactly that many zeros into d_witness ((n, 49) uint8)."""
+        st = stream if stream is not None else torch.cuda.current_stream(self.device)
+        need = ctypes.c_size_t(0)
+        _lib.check(_lib.load().tg_witness_workspace_size(ctypes.byref(p), ctypes.byref(need)),
+                   "tg_witness_workspace_size")
+        if self._ws is None or self._ws.numel() < need.value:
+            self._ws = torch.empty(max(int(need.value), 256), dtype=torch.uint8,
+                                   device=self.device)
+        self.last_params = p
+        _lib.check(
+            _lib.load().tg_max_zeros_witness(
+                self.ctx.handle, ctypes.byref(p), d_indices.data_ptr(), d_offsets.data_ptr(),
+                d_target.data_ptr() if d_target is not None else None, None,
+                d_out.data_ptr(), d_witness.data_ptr(), self._ws.data_ptr(), self._ws.numel(),
+                st.cuda_stream,
+            ),
+            "tg_max_zeros_witness",
+        )
+
     def status(self, p: _lib.DistanceParams, stream: torch.cuda.Stream) -> int:
         s = ctypes.c_int32(0)
         _lib.check(_lib.load().tg_distance_status(ctypes.byref(p), self._ws.data_ptr(),
@@ -349,6 +373,49 @@ class DistanceOracleCUDABP:
         if num_sets == 0:
             return []
         return self._evaluate(batched_indices, target_distance, sample_count, sample_seed)
+
+    def max_zeros_batch_witness(self, batched_indices, target_distance):
+        """max_zeros_batch (exact) plus one witness codeword per set.
+
+        Returns (values, witnesses): witnesses is an (n, 49) uint8 array of
+        GF(8) symbols in M's column order, row s a codeword of set s's code
+        with exactly values[s] zero coordinates (a minimum-weight codeword
+        when the set passes, a codeword below the target distance when it
+        fails; the zero codeword for dependent rows).  The reference returns
+        only the counts; a caller can check a witness on the host by solving
+        m M[S] = c."""
+        n = len(batched_indices)
+        if n == 0:
+            return [], np.zeros((0, N_POINTS), dtype=np.uint8)
+        flat, offsets, k_max = pack_sets(batched_indices)
+        if k_max > MAX_EXACT_K:
+            raise ValueError("Exact CUDA-BP batch evaluation supports k <= 21")
+        if flat.size and (int(flat.min()) < 0 or int(flat.max()) >= N_POINTS):
+            raise ValueError("exponent indices must lie in 0..48")
+        per_set_td = not np.isscalar(target_distance)
+        with self._lock, torch.cuda.device(self.device):
+            s = self._stream
+            with torch.cuda.stream(s):
+                d_idx = torch.from_numpy(flat if flat.size else np.zeros(1, np.int32)).to(
+                    self.device)
+                d_off = torch.from_numpy(offsets).to(self.device)
+                d_td = None
+                if per_set_td:
+                    td_arr = np.asarray(target_distance, dtype=np.int32)
+                    if td_arr.shape != (n,):
+                        raise ValueError("target_distance must be an int or one value per set")
+                    d_td = torch.from_numpy(td_arr).to(self.device)
+                d_out = torch.empty(n, dtype=torch.int32, device=self.device)
+                d_wit = torch.empty((n, N_POINTS), dtype=torch.uint8, device=self.device)
+                runner = self._runner_for(k_max, False)
+                p = runner.params(n, k_max, 0 if per_set_td else int(target_distance))
+                runner.run_witness(p, d_idx, d_off, d_out, d_wit, d_target=d_td, stream=s)
+                h_out = d_out.to("cpu", non_blocking=True)
+                h_wit = d_wit.to("cpu", non_blocking=True)
+            status = runner.status(p, s)  # synchronises the stream
+        if status != _lib.TG_OK:
+            _lib.check(status, "max_zeros_batch_witness (device)")
+        return h_out.tolist(), h_wit.numpy()
 
     def min_distance(self, s_indices: list[int], target_distance: int = 1) -> int:
         """49 - max_zeros (the helper of kernel backup.py:161-163)."""

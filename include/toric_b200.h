@@ -169,6 +169,29 @@ int tg_max_zeros_walk_part(tg_context* ctx, const tg_distance_params* p,
                            int32_t parts, int32_t* d_out, void* d_workspace,
                            size_t workspace_bytes, void* stream);
 
+/* Bytes of workspace tg_max_zeros_witness needs (exact parameters only). */
+int tg_witness_workspace_size(const tg_distance_params* p, size_t* h_bytes);
+
+/* tg_max_zeros plus, for every set, a witness codeword: 49 GF(8) symbols
+ * (uint8, values 0..7, in M's column order) at d_witness + 49 * s, with
+ * exactly d_out[s] zero coordinates.  For a passing set it is a codeword of
+ * minimum weight; for a failing set one of weight below the target
+ * distance, whose zero count d_out[s] then reports (still > 49 - td).  A set
+ * with dependent rows gets the zero codeword (d_out = 49); an empty set
+ * gets zeros.  The reference returns only the count
+ * (DistanceOracleCUDABP.max_zeros_batch, kernel_cuda_bp.py:290-323; its
+ * message poly_id stays inside eval_min_distance_batch_bp :146-238); the
+ * witness lets a caller check a result on the host by solving m M[S] = c.
+ * Runs a second information-set pass whose per-set targets are 50 - d_out,
+ * recording the first codeword that reaches them; a set evaluated by the walk
+ * without a witness raises TG_ERR_STATE through tg_distance_status (same
+ * workspace).  Exact parameters only (sample_count == 0). */
+int tg_max_zeros_witness(tg_context* ctx, const tg_distance_params* p,
+                         const int32_t* d_indices, const int64_t* d_offsets,
+                         const int32_t* d_target, const int32_t* d_set_ids,
+                         int32_t* d_out, uint8_t* d_witness, void* d_workspace,
+                         size_t workspace_bytes, void* stream);
+
 /* Size of the library-owned scratch area tg_max_zeros_noalloc works in. */
 #define TG_STATIC_WORKSPACE_BYTES (16u << 20)
 

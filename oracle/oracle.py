@@ -54,6 +54,8 @@ def load():
         lib.or_eval_prefix_batch.restype = c_int64
         lib.or_eval_prefix_batch.argtypes = [c_void_p, c_void_p, c_void_p, c_int, c_uint64, c_int,
                                              c_void_p]
+        lib.or_codeword_message.restype = c_int
+        lib.or_codeword_message.argtypes = [c_void_p, c_void_p, c_int, c_void_p, c_void_p]
         lib.or_canonical_keys.restype = None
         lib.or_canonical_keys.argtypes = [c_void_p, c_int, c_int, c_void_p, c_void_p, c_int]
         lib.or_canonical_masks.restype = None
@@ -159,6 +161,21 @@ def eval_prefix_batch(M, batched, count: int, threads: int = 0) -> tuple[int, li
     if msgs < 0:
         raise RuntimeError("oracle allocation failed")
     return int(msgs), out[:n].tolist()
+
+
+def codeword_message(M, S, codeword) -> tuple[int, list[int]]:
+    """Checks a witness codeword of the code M[S]: returns (zeros, message)
+    with message . M[S] == codeword recomputed by the oracle, or raises
+    ValueError when the codeword is not in the code (or is the zero codeword
+    of a code whose rows are independent)."""
+    M = np.ascontiguousarray(np.asarray(M, dtype=np.int32))
+    s = np.ascontiguousarray(np.asarray(S, dtype=np.int32))
+    cw = np.ascontiguousarray(np.asarray(codeword, dtype=np.uint8).reshape(NP))
+    msg = np.zeros(max(len(S), 1), dtype=np.int32)
+    z = load().or_codeword_message(_ptr(M), _ptr(s), len(S), _ptr(cw), _ptr(msg))
+    if z < 0:
+        raise ValueError(f"not a codeword of the set's code (status {z})")
+    return int(z), msg[:len(S)].tolist()
 
 
 def bf_max_zeros(S, M) -> int:

@@ -373,3 +373,77 @@ void or_canonical_masks(const uint64_t* masks, int n, uint64_t* out, int threads
     out[s] = best;
   }
 }
+
+/* ---- witness check (a test helper with no reference counterpart) ---------
+ * Solves m A = c over GF(8) for A = M[S] (k x 49 rows of the code) by
+ * Gauss-Jordan elimination of the 49 x (k + 1) system A^T m^T = c^T.  When c
+ * is a codeword it writes a message m with m A = c (nonzero whenever one
+ * exists: for c = 0 a null-space vector of a rank-deficient A), recomputes
+ * m A with the reference's evaluation (kernel.py:97-203: the sum over i of
+ * coefficient m_i times row S[i]) and returns the zero count of c.  Returns
+ * -1 when c is not in the row space or the recomputed codeword differs, -2
+ * when c = 0 and A has full rank (no nonzero message gives it), -3 for k out
+ * of 1..49. */
+int or_codeword_message(const int32_t* M, const int32_t* S, int k, const uint8_t* cw,
+                        int32_t* msg) {
+  init_mul();
+  if (k < 1 || k > NP) return -3;
+  uint8_t inv[8] = {0};
+  for (int a = 1; a < 8; ++a)
+    for (int b = 1; b < 8; ++b)
+      if (MUL[a * 8 + b] == 1) inv[a] = (uint8_t)b;
+  uint8_t E[NP][NP + 1];
+  for (int j = 0; j < NP; ++j) {
+    for (int i = 0; i < k; ++i) E[j][i] = (uint8_t)M[S[i] * NP + j];
+    E[j][k] = cw[j];
+  }
+  int pivrow_col[NP];
+  int is_pivot[NP];
+  for (int i = 0; i < k; ++i) is_pivot[i] = 0;
+  int r = 0;
+  for (int i = 0; i < k && r < NP; ++i) {
+    int p = -1;
+    for (int j = r; j < NP; ++j)
+      if (E[j][i]) { p = j; break; }
+    if (p < 0) continue;
+    if (p != r)
+      for (int t = 0; t <= k; ++t) { uint8_t x = E[p][t]; E[p][t] = E[r][t]; E[r][t] = x; }
+    const uint8_t s = inv[E[r][i]];
+    for (int t = 0; t <= k; ++t) E[r][t] = MUL[s * 8 + E[r][t]];
+    for (int j = 0; j < NP; ++j) {
+      if (j == r || !E[j][i]) continue;
+      const uint8_t f = E[j][i];
+      for (int t = 0; t <= k; ++t) E[j][t] ^= MUL[f * 8 + E[r][t]];
+    }
+    pivrow_col[r] = i;
+    is_pivot[i] = 1;
+    ++r;
+  }
+  for (int j = r; j < NP; ++j)
+    if (E[j][k]) return -1;  /* inconsistent: c is not a codeword */
+  int all_zero = 1;
+  for (int j = 0; j < NP; ++j)
+    if (cw[j]) all_zero = 0;
+  for (int i = 0; i < k; ++i) msg[i] = 0;
+  if (all_zero) {
+    int f = -1;
+    for (int i = 0; i < k && f < 0; ++i)
+      if (!is_pivot[i]) f = i;
+    if (f < 0) return -2;
+    msg[f] = 1;
+  }
+  for (int rr = 0; rr < r; ++rr) {
+    uint8_t v = E[rr][k];
+    for (int i = 0; i < k; ++i)
+      if (!is_pivot[i] && msg[i]) v ^= MUL[E[rr][i] * 8 + msg[i]];
+    msg[pivrow_col[rr]] = v;
+  }
+  int zeros = 0;
+  for (int j = 0; j < NP; ++j) {
+    uint8_t v = 0;
+    for (int i = 0; i < k; ++i) v ^= MUL[msg[i] * 8 + M[S[i] * NP + j]];
+    if (v != cw[j]) return -1;
+    if (v == 0) ++zeros;
+  }
+  return zeros;
+}
