@@ -83,6 +83,27 @@ def test_threshold_decisions_vs_reference_kernel(ref, dev_M, gpu_oracle, k, td):
             assert a == b == e
 
 
+@pytest.mark.parametrize("k", [10, 11])
+def test_default_path_vs_reference_kernel_large_k(ref, dev_M, gpu_oracle, k):
+    """The default enumeration (information sets for k >= 2) against the
+    reference kernel at the sizes that carry the batched mixed-k workload: 148
+    seeded sets (one reference block per SM), exact values, then pass/fail
+    decisions at target distances 20 and 25 (exact values for passing sets)."""
+    rng = np.random.default_rng(4100 + k)
+    sets = [sorted(rng.choice(N, k, replace=False).tolist()) for _ in range(148)]
+    exact = ref_batch(ref, dev_M, sets, 1)
+    assert gpu_oracle.max_zeros_batch(sets, 1) == exact
+    for td in (20, 25):
+        tmax = N - td
+        ours = gpu_oracle.max_zeros_batch(sets, td)
+        theirs = ref_batch(ref, dev_M, sets, td) if k == 10 else exact
+        for e, a, b in zip(exact, ours, theirs):
+            assert (a > tmax) == (b > tmax) == (e > tmax)
+            if e <= tmax:
+                assert a == b == e
+    assert len(set(exact)) > 1
+
+
 @pytest.mark.parametrize("k", [4, 11, 15, 21, 22, 33, 49])
 def test_sampled_vs_reference_kernel(ref, dev_M, gpu_oracle, k):
     rng = random.Random(700 + k)

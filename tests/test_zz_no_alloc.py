@@ -99,3 +99,23 @@ def test_noalloc_rejects_oversized_batch(env):
                                   dummy.data_ptr(), None, None, dummy.data_ptr(), None)
     assert st == _lib.TG_ERR_WORKSPACE
     assert "static workspace" in _lib.last_error()
+
+
+def test_noalloc_out_of_range_set_reads_zero(env):
+    """A set with an index outside 0..48 comes back as 0 from the zero-allocation
+    entry point (it has no status query); the other sets of the batch keep the
+    values a clean batch gives them.  The allocating entry point gives the
+    same values (and reports the set through tg_distance_status)."""
+    rng = random.Random(91)
+    clean = [sorted(rng.sample(range(49), rng.randint(3, 10))) for _ in range(30)]
+    bad = [list(s) for s in clean]
+    bad[7] = bad[7][:-1] + [49]
+    bad[19] = [-1] + bad[19][1:]
+    want, want_static = _run_both(env, clean, 1)
+    assert want == want_static
+    got, got_static = _run_both(env, bad, 1)
+    for i in range(len(clean)):
+        if i in (7, 19):
+            assert got[i] == 0 and got_static[i] == 0
+        else:
+            assert got[i] == want[i] and got_static[i] == want[i]
