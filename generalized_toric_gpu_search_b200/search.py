@@ -13,14 +13,18 @@ level is five device steps with no host round trip but one count:
   (torch compare)       survivors by the keep threshold
 
 `CanonicalBFS.run` drives levels like `canonical_champion_search`
-(:386-604) and yields, per level, the canonical sets, their max_zeros and the
-survivors; `records` renders the reference's JSONL record shapes.
+(:386-604) -- targets, prune margin and evaluation mode, sampled screening,
+resume -- and yields, per level, the canonical sets and their max_zeros;
+`level_records` / `append_records` / `load_canonical_state` write and read
+the reference's JSONL results file, so either side resumes the other's run.
 """
 
 from __future__ import annotations
 
 import ctypes
+import json
 from dataclasses import dataclass
+from pathlib import Path
 
 import numpy as np
 import torch
@@ -28,7 +32,8 @@ import torch
 from . import _lib
 from .canonical import CanonicalDedup
 from .distance import DistanceRunner, LaunchConfig, ToricContext
-from .tables import N_POINTS, bounding_cube_points, build_eval_matrix, indices_of, pack_canonical
+from .tables import (N_POINTS, bounding_cube_points, build_eval_matrix, indices_of, mask_of,
+                     pack_canonical, unpack_canonical)
 
 
 @dataclass
@@ -114,43 +119,182 @@ class CanonicalBFS:
         self.stream.synchronize()
         return Level(k, masks, sets, mz, eval_distance)
 
-    def run(self, max_k: int, targets: dict[int, int], prune_margin: int | None = None):
-        """Yields Level objects for k = 2..max_k, keeping every class
-        (prune_margin None) or those with d >= targets[k] - prune_margin, as
-        the reference's canonical_champion_search does (champion mode)."""
-        parents = self.first_level()
-        for k in range(2, max_k + 1):
-            td = targets.get(k, 1)
-            lv = self.level(parents, k, td)
+    def evaluate_sampled(self, sets: torch.Tensor, offsets: torch.Tensor, k: int,
+                         target_distance: int, sample_count: int, sample_seed: int,
+                         batch_size: int) -> torch.Tensor:
+        """Sampled screening of a level, as the reference's driver batches it:
+        set j of the level is position j % batch_size of its batch, the
+        sampling id of the reference kernel (blockIdx.x), with the level's
+        seed."""
+        m = sets.shape[0]
+        out = torch.empty(max(m, 1), dtype=torch.int32, device=self.device)
+        if m:
+            ids = (torch.arange(m, dtype=torch.int32, device=self.device) % batch_size)
+            p = self.runner.params(m, k, target_distance, sample_count, sample_seed)
+            with torch.cuda.stream(self.stream):
+                self.runner.run(p, sets, offsets, out, d_set_ids=ids, stream=self.stream)
+        return out[:m]
+
+    def run(self, max_k: int, targets: dict[int, int], prune_margin: int | None = None, *,
+            prune_eval_mode: str = "champion", screen_from_k: int | None = None,
+            screen_sample_count: int = 0, screen_seed: int = 1, batch_size: int = 50_000,
+            results_file: Path | str | None = None, resume: bool = True,
+            screen_candidate_log_limit: int = 200, lattice=None):
+        """Yields Level objects for the levels up to max_k, following
+        canonical_champion_search (champion_search_canonical.py:386-604):
+        per level k the target td = targets[k], keep distance and evaluation
+        distance from prune_margin / prune_eval_mode, sampled screening for
+        k >= screen_from_k, survivors (every class when prune_margin is None,
+        else those with d >= keep distance) as the next level's parents.
+        With results_file, the level's records are appended in the
+        reference's JSONL format, and a run resumes after the last completed
+        level of that file (load_canonical_state)."""
+        if prune_eval_mode not in ("champion", "survivor"):
+            raise ValueError("prune_eval_mode must be 'champion' or 'survivor'")
+        path = Path(results_file) if results_file is not None else None
+        lattice = lattice if lattice is not None else bounding_cube_points()
+        start_k, packed0 = 1, {0}
+        if path is not None and resume and path.exists():
+            start_k, packed0 = load_canonical_state(path)
+        masks0 = sorted(mask_of(unpack_canonical(p, start_k)) for p in packed0)
+        parents = torch.tensor(masks0, dtype=torch.int64, device=self.device)
+        for k in range(start_k + 1, max_k + 1):
+            if parents.numel() == 0:
+                return
+            td, keep_distance, eval_distance, sample_count = level_settings(
+                k, targets, prune_margin, prune_eval_mode, screen_from_k, screen_sample_count)
+            masks, sets, offsets = self.expand(parents, k)
+            if sample_count > 0:
+                mz = self.evaluate_sampled(sets, offsets, k, eval_distance, sample_count,
+                                           screen_seed + k * 1_000_003, batch_size)
+            else:
+                mz = self.evaluate(sets, offsets, k, eval_distance)
+            self.stream.synchronize()
+            lv = Level(k, masks, sets, mz, eval_distance)
+            if path is not None:
+                h_masks, _, h_mz = lv.host()
+                packed = [pack_canonical(indices_of(int(m))) for m in h_masks.tolist()]
+                indices = [indices_of(int(m)) for m in h_masks.tolist()]
+                recs, _ = level_records(k, packed, indices, h_mz.tolist(), lattice, td,
+                                        prune_margin=prune_margin,
+                                        prune_eval_mode=prune_eval_mode,
+                                        sample_count=sample_count,
+                                        screen_candidate_log_limit=screen_candidate_log_limit)
+                append_records(recs, path)
             yield lv
             if prune_margin is None:
                 parents = lv.masks
             else:
-                keep = max(1, td - prune_margin)
-                parents = lv.masks[lv.max_zeros <= N_POINTS - keep]
-            if parents.numel() == 0:
-                return
+                parents = lv.masks[lv.max_zeros <= N_POINTS - keep_distance]
 
 
-def records(level: Level, best_known_d: int) -> list[dict]:
-    """The reference's JSONL records for a level (champion_search_canonical.py:536-583):
-    champions (d >= best_known_d), one survivor record per class, the sentinel."""
-    masks, sets, mz = level.host()
-    lattice = bounding_cube_points()
-    out = []
+# ---------------------------------------------------------------------------
+# The reference's JSONL records (host side)
+# ---------------------------------------------------------------------------
+
+def level_settings(k: int, targets: dict[int, int], prune_margin: int | None,
+                   prune_eval_mode: str, screen_from_k: int | None,
+                   screen_sample_count: int) -> tuple[int, int, int, int]:
+    """(td, keep_distance, eval_distance, sample_count) of level k
+    (champion_search_canonical.py:479-491)."""
+    td = targets.get(k, 1)
+    keep_distance = 1 if prune_margin is None else max(1, td - prune_margin)
+    eval_distance = td if prune_margin is None or prune_eval_mode == "champion" else keep_distance
+    sample_count = screen_sample_count if screen_from_k is not None and k >= screen_from_k else 0
+    return td, keep_distance, eval_distance, sample_count
+
+
+def level_records(k: int, packed, indices, max_zeros, lattice, td: int, *,
+                  prune_margin: int | None = None, prune_eval_mode: str = "champion",
+                  sample_count: int = 0, screen_candidate_log_limit: int = 200
+                  ) -> tuple[list[dict], list[int]]:
+    """The records canonical_champion_search appends for one level, in its
+    order and key order (champion_search_canonical.py:531-583), and the
+    packed keys the level keeps as survivors:
+      * a champion record per set with d >= td on an exact level;
+      * on a screened level instead up to screen_candidate_log_limit
+        unverified candidate records;
+      * a survivor record per kept set (all sets when prune_margin is None,
+        else those with d >= max(1, td - prune_margin));
+      * the level_complete sentinel.
+    packed, indices and max_zeros are the level's sets in evaluation order."""
+    _, keep_distance, eval_distance, _ = level_settings(k, {k: td}, prune_margin,
+                                                        prune_eval_mode, None, 0)
+    screened = sample_count > 0
+    out: list[dict] = []
+    kept: list[int] = []
+    seen_kept: set[int] = set()
     n_champ = 0
-    for m, row, z in zip(masks.tolist(), sets.tolist(), mz.tolist()):
-        d = N_POINTS - int(z)
-        if d >= best_known_d:
+    n_logged = 0
+    for p, S, mz in zip(packed, indices, max_zeros):
+        mz = int(mz)
+        d = N_POINTS - mz
+        S = [int(i) for i in S]
+        if d >= td and not screened:
             n_champ += 1
-            out.append({"name": f"canon_k{level.k}_d{d}", "indices": list(row),
-                        "lattice_points": [list(lattice[i]) for i in row], "k": level.k,
-                        "max_zeros": int(z), "min_distance": d, "best_known_d": best_known_d,
-                        "new_record": d > best_known_d})
-    for m in masks.tolist():
-        out.append({"type": "survivor", "k": level.k,
-                    "packed": pack_canonical(indices_of(int(m)))})
-    out.append({"type": "level_complete", "k": level.k, "n_canonical": len(masks),
-                "n_champions": n_champ, "n_survivors": len(masks),
-                "eval_distance": level.eval_distance, "verified": True})
+            out.append({"name": f"canon_k{k}_d{d}", "indices": S,
+                        "lattice_points": [list(lattice[i]) for i in S], "k": k,
+                        "max_zeros": mz, "min_distance": d, "best_known_d": td,
+                        "new_record": d > td})
+        elif d >= td and screened and n_logged < screen_candidate_log_limit:
+            n_logged += 1
+            out.append({"type": "candidate", "verified": False,
+                        "name": f"screen_k{k}_sample_d{d}", "indices": S,
+                        "lattice_points": [list(lattice[i]) for i in S], "k": k,
+                        "sampled_max_zeros": mz, "sampled_min_distance": d, "best_known_d": td,
+                        "sample_count": sample_count})
+        if prune_margin is None or d >= keep_distance:
+            if p not in seen_kept:
+                seen_kept.add(p)
+                kept.append(p)
+            out.append({"type": "survivor", "k": k, "packed": int(p)})
+    out.append({"type": "level_complete", "k": k, "n_canonical": len(packed),
+                "n_champions": n_champ, "n_survivors": len(kept),
+                "prune_eval_mode": prune_eval_mode, "eval_distance": eval_distance,
+                "keep_distance": keep_distance, "screen_sample_count": sample_count,
+                "verified": not screened})
+    return out, kept
+
+
+def append_records(records, path: Path | str) -> None:
+    """Appends records as JSON lines (champion_search_canonical.py:168-170)."""
+    with Path(path).open("a") as f:
+        for r in records:
+            f.write(json.dumps(r) + "\n")
+
+
+def load_canonical_state(path: Path | str) -> tuple[int, set[int]]:
+    """(last completed k, packed survivors of that level) of a results file,
+    or (1, {0}) when it holds no completed level -- the resume rule of
+    champion_search_canonical.py:190-210, so a device-BFS run and the
+    reference driver resume each other's files."""
+    path = Path(path)
+    survivors: dict[int, set[int]] = {}
+    completed: set[int] = set()
+    if path.exists():
+        for line in path.read_text().splitlines():
+            line = line.strip()
+            if not line:
+                continue
+            rec = json.loads(line)
+            if rec.get("type") == "level_complete":
+                completed.add(rec["k"])
+            elif rec.get("type") == "survivor":
+                survivors.setdefault(rec["k"], set()).add(rec["packed"])
+    if not completed:
+        return 1, {0}
+    last = max(completed)
+    return last, survivors.get(last, set())
+
+
+def records(level: Level, best_known_d: int, prune_margin: int | None = None,
+            prune_eval_mode: str = "champion", sample_count: int = 0) -> list[dict]:
+    """The reference's JSONL records of a device-BFS level (level_records on
+    its canonical sets, in the level's order)."""
+    masks, _, mz = level.host()
+    packed = [pack_canonical(indices_of(int(m))) for m in masks.tolist()]
+    indices = [indices_of(int(m)) for m in masks.tolist()]
+    out, _ = level_records(level.k, packed, indices, mz.tolist(), bounding_cube_points(),
+                           best_known_d, prune_margin=prune_margin,
+                           prune_eval_mode=prune_eval_mode, sample_count=sample_count)
     return out
