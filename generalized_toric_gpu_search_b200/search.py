@@ -206,8 +206,8 @@ def level_settings(k: int, targets: dict[int, int], prune_margin: int | None,
 
 def level_records(k: int, packed, indices, max_zeros, lattice, td: int, *,
                   prune_margin: int | None = None, prune_eval_mode: str = "champion",
-                  sample_count: int = 0, screen_candidate_log_limit: int = 200
-                  ) -> tuple[list[dict], list[int]]:
+                  sample_count: int = 0, screen_candidate_log_limit: int = 200,
+                  eval_distance: int | None = None) -> tuple[list[dict], list[int]]:
     """The records canonical_champion_search appends for one level, in its
     order and key order (champion_search_canonical.py:531-583), and the
     packed keys the level keeps as survivors:
@@ -217,9 +217,13 @@ def level_records(k: int, packed, indices, max_zeros, lattice, td: int, *,
       * a survivor record per kept set (all sets when prune_margin is None,
         else those with d >= max(1, td - prune_margin));
       * the level_complete sentinel.
-    packed, indices and max_zeros are the level's sets in evaluation order."""
-    _, keep_distance, eval_distance, _ = level_settings(k, {k: td}, prune_margin,
-                                                        prune_eval_mode, None, 0)
+    packed, indices and max_zeros are the level's sets in evaluation order;
+    eval_distance, when given, is the distance the level was evaluated at
+    (else the driver's rule derives it from td and the prune settings)."""
+    _, keep_distance, derived_eval, _ = level_settings(k, {k: td}, prune_margin,
+                                                       prune_eval_mode, None, 0)
+    if eval_distance is None:
+        eval_distance = derived_eval
     screened = sample_count > 0
     out: list[dict] = []
     kept: list[int] = []
@@ -296,5 +300,6 @@ def records(level: Level, best_known_d: int, prune_margin: int | None = None,
     indices = [indices_of(int(m)) for m in masks.tolist()]
     out, _ = level_records(level.k, packed, indices, mz.tolist(), bounding_cube_points(),
                            best_known_d, prune_margin=prune_margin,
-                           prune_eval_mode=prune_eval_mode, sample_count=sample_count)
+                           prune_eval_mode=prune_eval_mode, sample_count=sample_count,
+                           eval_distance=level.eval_distance)
     return out

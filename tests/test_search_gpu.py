@@ -37,7 +37,7 @@ def test_bfs_levels_cover_every_class(canon_oracle, M):
     recs = records(levels[1], best_known_d=40)
     assert recs[-1] == {"type": "level_complete", "k": 3, "n_canonical": 3, "n_champions":
                         sum(1 for r in recs if "name" in r), "n_survivors": 3,
-                        "prune_eval_mode": "champion", "eval_distance": 40,
+                        "prune_eval_mode": "champion", "eval_distance": 1,
                         "keep_distance": 1, "screen_sample_count": 0, "verified": True}
     torch.cuda.synchronize()
 
