@@ -557,9 +557,11 @@ __device__ __noinline__ int is_sweep_exact_w(V6 P, const V6* g_row, int wmin, Wi
 }
 
 // Exact weights of the seven codewords P + alpha^v g, v = 0..6, min'd into
-// wmin.
+// wmin (kCG: g_row may have been written during the kernel, so it is read
+// through L2 only).
+template <bool kCG>
 __device__ __noinline__ int is_sweep_exact(V6 P, const V6* g_row, int wmin) {
-  V6 g = v6_ldg(g_row);
+  V6 g = v6_load<kCG>(g_row);
   for (int v = 0; v < 7; ++v) {
     const int lo = __popc(lop3<0xFE>(P.l0 ^ g.l0, P.l1 ^ g.l1, P.l2 ^ g.l2));
     const int hi = __popc(lop3<0xFE>(P.h0 ^ g.h0, P.h1 ^ g.h1, P.h2 ^ g.h2));
@@ -647,17 +649,19 @@ __device__ __noinline__ void is_sweep_witness(Pl3 W, Pl3 Pz, const V6* g_row, in
   is_put_witness(wo, P.x0 ^ gl.x0, P.x1 ^ gl.x1, P.x2 ^ gl.x2, ph0 ^ gh0, ph1 ^ gh1, ph2 ^ gh2);
 }
 
-template <bool kW>
+template <bool kW, bool kCG>
 __device__ __forceinline__ int is_sweep_fix(uint32_t kC, const int (&z)[7], int zz, uint32_t ph0,
                                             uint32_t ph1, uint32_t ph2, const V6* g_row,
                                             const V6* r1_row, int wmin, const Pl3& W,
                                             const Pl3& Pz, WitOut wo, int wthr) {
-  uint32_t d0 = __ldg(&r1_row->h0), d1 = __ldg(&r1_row->h1), d2 = __ldg(&r1_row->h2);
+  uint32_t d0 = ld_u32<kCG>(&r1_row->h0), d1 = ld_u32<kCG>(&r1_row->h1),
+           d2 = ld_u32<kCG>(&r1_row->h2);
   gf8_scale32(kC, d0, d1, d2);
   ph0 ^= d0;
   ph1 ^= d1;
   ph2 ^= d2;
-  uint32_t g0 = __ldg(&g_row->h0), g1 = __ldg(&g_row->h1), g2 = __ldg(&g_row->h2);
+  uint32_t g0 = ld_u32<kCG>(&g_row->h0), g1 = ld_u32<kCG>(&g_row->h1),
+           g2 = ld_u32<kCG>(&g_row->h2);
   const int lo_base = 32 - zz;
 #pragma unroll
   for (int v = 0; v < 7; ++v) {
@@ -701,8 +705,8 @@ __device__ __forceinline__ int is_sweep_fix(uint32_t kC, const int (&z)[7], int 
     const int zm_ = __vimax3_s32(__vimax3_s32(z_[0], z_[1], z_[2]),                              \
                                  __vimax3_s32(z_[3], z_[4], z_[5]), z_[6]) - pz_;                \
     if (__builtin_expect(zm_ > thz, 0)) {                                                        \
-      wmin = is_sweep_fix<kW>(kC, z_, ngz - pz_, qh0, qh1, qh2, rows + r0, rows + r1, wmin, W,   \
-                              Pz, wo, wthr);                                                     \
+      wmin = is_sweep_fix<kW, kCG>(kC, z_, ngz - pz_, qh0, qh1, qh2, rows + r0, rows + r1, wmin, \
+                                   W, Pz, wo, wthr);                                             \
       thz = thz_base - wmin;                                                                     \
     }                                                                                            \
   }
@@ -736,7 +740,7 @@ __device__ __forceinline__ int is_sweep_fix(uint32_t kC, const int (&z)[7], int 
 // W and Pz are the state of sweep 6; stepping back through digit 1's moves
 // (ez, stride kStride) gives each earlier sweep's.  Sweep s has digit 1 at
 // alpha^s (alpha^0..6 = 1, 2, 4, 3, 6, 7, 5, packed in nibbles).
-template <int kStride, bool kW>
+template <int kStride, bool kW, bool kCG>
 __device__ __forceinline__ int is_block_fix(unsigned fl, Pl3 W, Pl3 Pz, const uint32_t* ez, int ngz,
                                          uint32_t qh0, uint32_t qh1, uint32_t qh2,
                                          const V6* g_row, const V6* r1_row, int wmin, WitOut wo,
@@ -745,7 +749,7 @@ __device__ __forceinline__ int is_block_fix(unsigned fl, Pl3 W, Pl3 Pz, const ui
     if ((fl >> s) & 1u) {
       TG_IS_ZCOUNTS(z_)
       const int pz_ = __popc(lop3<0xFE>(Pz.x0, Pz.x1, Pz.x2));
-      wmin = is_sweep_fix<kW>((0x05763421u >> (4 * s)) & 0xFu, z_, ngz - pz_, qh0, qh1, qh2,
+      wmin = is_sweep_fix<kW, kCG>((0x05763421u >> (4 * s)) & 0xFu, z_, ngz - pz_, qh0, qh1, qh2,
                               g_row, r1_row, wmin, W, Pz, wo, wthr);
       fl &= ~(1u << s);
     }
@@ -779,19 +783,19 @@ constexpr int kIsPairThr = 15;
 // P's high word without digit 1's term (qh, which only the block moves
 // change) is kept for the exact count of a rare sweep.  Returns the codewords
 // evaluated.
-template <int kStride, bool kW>
+template <int kStride, bool kW, bool kCG>
 __device__ __forceinline__ unsigned long long is_walk_blocks(
     const V6& P, const V6* rows, uint32_t r0, uint32_t r1, const uint16_t* dig, uint32_t* ez,
     unsigned long long b0, unsigned long long nblk, int hb, int wthr, const int32_t* stop,
     int& wmin, WitOut wo) {
-  const Pl3 g = pl3_lo(v6_ldg(rows + r0));
+  const Pl3 g = pl3_lo(v6_load<kCG>(rows + r0));
   const Pl3 h = pl3_inv(g);
   const uint32_t gz = ~(g.x0 | g.x1 | g.x2);  // low columns where g is 0
   const int ngz = __popc(gz);
   // Digit 1's step i is (alpha^i + alpha^(i+1)) r1 = alpha^i (1 + alpha) r1:
   // one product with h for the first, then a multiplication by alpha (one
   // XOR) for each next, in both domains.
-  const Pl3 d0 = pl3_lo(v6_ldg(rows + r1 + 1));
+  const Pl3 d0 = pl3_lo(v6_load<kCG>(rows + r1 + 1));
   Pl3 e = pl3_mul(d0, h);
   Pl3 zq = pl3_and(d0, gz);
 #pragma unroll
@@ -807,7 +811,7 @@ __device__ __forceinline__ unsigned long long is_walk_blocks(
   }
   {
     // (alpha^6 + alpha^0) r1 = alpha^2 r1
-    const Pl3 r = pl3_lo(v6_ldg(rows + r1));
+    const Pl3 r = pl3_lo(v6_load<kCG>(rows + r1));
     ez[36 * kStride] = r.x1;
     ez[37 * kStride] = r.x1 ^ r.x2;
     ez[38 * kStride] = r.x0 ^ r.x2;
@@ -815,9 +819,9 @@ __device__ __forceinline__ unsigned long long is_walk_blocks(
   Pl3 W = pl3_mul(pl3_lo(P), h);
   Pl3 Pz = pl3_and(pl3_lo(P), gz);
   // digit 1 starts at alpha^0
-  uint32_t qh0 = P.h0 ^ __ldg(&rows[r1].h0);
-  uint32_t qh1 = P.h1 ^ __ldg(&rows[r1].h1);
-  uint32_t qh2 = P.h2 ^ __ldg(&rows[r1].h2);
+  uint32_t qh0 = P.h0 ^ ld_u32<kCG>(&rows[r1].h0);
+  uint32_t qh1 = P.h1 ^ ld_u32<kCG>(&rows[r1].h1);
+  uint32_t qh2 = P.h2 ^ ld_u32<kCG>(&rows[r1].h2);
   const int thz_base = 32 + hb - ngz;
   int thz = thz_base - wmin;
   // The move into block m = b0 + i + 1 changes digit 2 when m % 7 != 0 (six
@@ -828,7 +832,7 @@ __device__ __forceinline__ unsigned long long is_walk_blocks(
   int par = int(((b0 + 1ull) / 7ull) & 1ull);
   V6 nx;
   v6_zero(nx);
-  if (n > 1) nx = v6_ldg(is_block_move<kStride>(rows, dig, b0 + 1ull));
+  if (n > 1) nx = v6_load<kCG>(is_block_move<kStride>(rows, dig, b0 + 1ull));
   int i = 0;
   for (; i < n; ++i) {
     if (i) {
@@ -849,7 +853,7 @@ __device__ __forceinline__ unsigned long long is_walk_blocks(
       if (i + 1 < n) {
         const V6* mv = m7 != 0 ? rows + dig[0] + 1 + (par ? 6 - m7 : m7 - 1)
                                : is_block_move<kStride>(rows, dig, b0 + unsigned(i) + 1ull);
-        nx = v6_ldg(mv);
+        nx = v6_load<kCG>(mv);
       }
     }
     // Sweep s at digit-1 coefficient alpha^s; the flagged ones are counted
@@ -867,7 +871,7 @@ __device__ __forceinline__ unsigned long long is_walk_blocks(
       TG_IS_SWEEP1(5, 7u); TG_IS_MOVE(5); TG_IS_SWEEP1(6, 5u);
     }
     if (__builtin_expect(fl != 0u, 0)) {
-      wmin = is_block_fix<kStride, kW>(fl, W, Pz, ez, ngz, qh0, qh1, qh2, rows + r0, rows + r1,
+      wmin = is_block_fix<kStride, kW, kCG>(fl, W, Pz, ez, ngz, qh0, qh1, qh2, rows + r0, rows + r1,
                                        wmin, wo, wthr);
       thz = thz_base - wmin;
     }
@@ -888,19 +892,30 @@ __device__ __forceinline__ unsigned long long is_walk_blocks(
 // smallest weight met (or wmin when none is smaller), and the codewords
 // evaluated in ncw.  dig and ez (stride kStride) are this thread's shared
 // scratch: the rows of digits 2..w-2 and digit 1's moves.
-template <int kStride, bool kW>
-__device__ __forceinline__ int is_walk_units(const DistArgs& a,
+// Where the witness pass of one code records its witness (pivot words of
+// its sets, output row, claim word); all NULL outside the witness pass.
+struct WitSrc {
+  const uint64_t* piv;
+  uint8_t* dst;
+  int32_t* lock;
+};
+
+// Units [u0, u1) of level w of one code whose information sets start at
+// `base` (n_sets sets of k rows, the last with rank deficit delta); `stop`
+// is the code's abort flag.  The smallest weight met (or wmin when none is
+// smaller), and the codewords evaluated in ncw.  dig and ez (stride kStride)
+// are this thread's shared scratch: the rows of digits 2..w-2 and digit 1's
+// moves.  Serves the batch walk and the served loop alike.
+template <int kStride, bool kW, bool kCG>
+__device__ __forceinline__ int is_walk_range(const V6* base, int n_sets, int delta,
+                                             const int32_t* stop, WitSrc wsrc,
                                              const unsigned long long (*bn)[kIsBinom],
-                                             uint16_t* dig, uint32_t* ez, int c, int k, int w,
+                                             uint16_t* dig, uint32_t* ez, int k, int w,
                                              unsigned long long u0, unsigned long long u1,
                                              int wthr, int wmin, unsigned long long& ncw) {
   const unsigned long long n_sup = bn[k][w];
   const unsigned long long bps = is_units_per_support(w);
   const unsigned long long per_set = n_sup * bps;
-  const V6* base = a.is_rows + size_t(c) * a.is_stride;
-  const int32_t* stop = a.abort + c;
-  const int n_sets = a.desc[c].H;
-  const int delta = a.desc[c].n_pat;  // rank deficit of the last set (0: full)
   ncw = 0ull;
   unsigned long long u = u0;
   while (u < u1) {
@@ -938,7 +953,7 @@ __device__ __forceinline__ int is_walk_units(const DistArgs& a,
       if (rem > 0 && q == 0) {
         r0 = R;
       } else {
-        V6 g = v6_ldg(rows + R);
+        V6 g = v6_load<kCG>(rows + R);
         if (rem > 0) {
           if (q == 1) {
             r1 = R;
@@ -956,7 +971,7 @@ __device__ __forceinline__ int is_walk_units(const DistArgs& a,
       wmin = min(wmin, wt);
       ncw += 1ull;
     } else if (w == 2) {
-      wmin = is_sweep_exact(P, rows + r0, wmin);
+      wmin = is_sweep_exact<kCG>(P, rows + r0, wmin);
       ncw += 7ull;
     } else {
       // Weight on the set's pivot columns: the message restricted to the rows
@@ -964,14 +979,30 @@ __device__ __forceinline__ int is_walk_units(const DistArgs& a,
       // that do not fit in the 17 high columns (k > 17).
       const int dj = int(j) == n_sets - 1 ? delta : 0;
       const int hb = max(0, w - dj - max(0, (k - dj) - 17));
-      const WitOut wo = kW ? wit_out(a, c, int(j)) : WitOut{nullptr, nullptr, nullptr};
-      ncw += is_walk_blocks<kStride, kW>(P, rows, r0, r1, dig, ez, b, nblk, hb, wthr, stop, wmin,
+      const WitOut wo = kW ? WitOut{wsrc.piv + j, wsrc.dst, wsrc.lock}
+                           : WitOut{nullptr, nullptr, nullptr};
+      ncw += is_walk_blocks<kStride, kW, kCG>(P, rows, r0, r1, dig, ez, b, nblk, hb, wthr, stop, wmin,
                                          wo);
     }
     u += nblk;
     if (wmin < wthr) break;
   }
   return wmin;
+}
+
+// is_walk_range for code c of a batch.
+template <int kStride, bool kW>
+__device__ __forceinline__ int is_walk_units(const DistArgs& a,
+                                             const unsigned long long (*bn)[kIsBinom],
+                                             uint16_t* dig, uint32_t* ez, int c, int k, int w,
+                                             unsigned long long u0, unsigned long long u1,
+                                             int wthr, int wmin, unsigned long long& ncw) {
+  const WitSrc wsrc = kW ? WitSrc{a.is_piv + size_t(c) * kIsMaxSets, a.witness + size_t(c) * kN,
+                                  a.wit_lock + c}
+                         : WitSrc{nullptr, nullptr, nullptr};
+  return is_walk_range<kStride, kW, false>(a.is_rows + size_t(c) * a.is_stride, a.desc[c].H,
+                                    a.desc[c].n_pat, a.abort + c, wsrc, bn, dig, ez, k, w, u0,
+                                    u1, wthr, wmin, ncw);
 }
 
 constexpr int kIsMaxDigits = kMaxExactK - 3;  // digits 2..w-2, w <= 21
@@ -1105,14 +1136,14 @@ __global__ void __launch_bounds__(128) levels123_kernel(DistArgs a) {
     const V6 Q = v6_ldg(rows + q * kIsVecPerRow);
     if (t < 0) {
       wmin = wit ? is_sweep_exact_w(Q, rows + p * kIsVecPerRow, wmin, wit_out(a, c, j), wthr)
-                 : is_sweep_exact(Q, rows + p * kIsVecPerRow, wmin);
+                 : is_sweep_exact<false>(Q, rows + p * kIsVecPerRow, wmin);
     } else {
       V6 X = v6_ldg(rows + p * kIsVecPerRow);  // alpha^s row_p, s = 0..6
       for (int s7 = 0; s7 < 7; ++s7) {
         V6 P = Q;
         v6_xor(P, X);
         wmin = wit ? is_sweep_exact_w(P, rows + t * kIsVecPerRow, wmin, wit_out(a, c, j), wthr)
-                   : is_sweep_exact(P, rows + t * kIsVecPerRow, wmin);
+                   : is_sweep_exact<false>(P, rows + t * kIsVecPerRow, wmin);
         v6_alpha_pow(X, 1);
       }
     }
