@@ -111,6 +111,7 @@ SIGNATURES: dict[str, tuple] = {
     "tg_server_poll": (c_int, [c_void_p, c_void_p, c_int32, POINTER(c_int32)]),
     "tg_server_stats": (c_int, [c_void_p, POINTER(c_uint64)]),
     "tg_server_destroy": (c_int, [c_void_p]),
+    "tg_server_debug_skip_publication": (c_int, [c_void_p]),
 }
 
 TG_RESULT_PASS = 1

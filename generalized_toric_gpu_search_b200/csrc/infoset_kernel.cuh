@@ -1087,38 +1087,30 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) walk_level_kernel(DistArgs a
   if (lane == 0 && evaluated) atomicAdd(&a.is_hdr->codewords, evaluated);
 }
 
-// Levels 1 to 3 of every set in one launch, one warp per set: the rows
-// themselves (weight-1 messages); for each pair of rows q < p the sweep
-// alpha^v row_p + row_q; and for each triple q < p < t the seven sweeps
-// alpha^v row_t + alpha^s row_p + row_q (messages up to scalars).  These
-// levels are too small to fill the GPU one launch each, and running them
-// without the bound check between them only adds codewords (the best weight
-// stays that of a codeword); level 4 onwards then follows the plan / scan /
-// walk triple.
-__global__ void __launch_bounds__(128) levels123_kernel(DistArgs a) {
-  const int lane = threadIdx.x & 31;
-  const int c = blockIdx.x * 4 + (threadIdx.x >> 5);
-  if (c >= a.n) return;  // warp-uniform
-  const CodeDesc d = a.desc[c];
-  if ((d.flags & kIsCodeFlag) == 0 || (d.flags & kDecidedFlag) != 0 || ld_flag(a.abort + c) != 0)
-    return;
-  const int k = d.k;
+// Levels 1 to 3 of n_sets information sets of k rows (at base), by one warp:
+// the rows themselves (weight-1 messages); for each pair of rows q < p the
+// sweep alpha^v row_p + row_q; for each triple q < p < t the seven sweeps
+// alpha^v row_t + alpha^s row_p + row_q (messages up to scalars).  Returns
+// the smallest weight, reduced over the warp; ncw = codewords evaluated.
+// With wsrc.dst set (the witness pass) the first codeword lighter than wthr
+// is recorded.  kCG: the rows may have been written during the launch.
+template <bool kCG>
+__device__ int is_levels123_sets(int lane, const V6* base, int n_sets, int k, WitSrc wsrc,
+                                 int wthr, unsigned long long& ncw) {
   const int n1 = k, n2 = k * (k - 1) / 2, n3 = k * (k - 1) * (k - 2) / 6;
   const int per_set = n1 + n2 + n3;
-  const int total = d.H * per_set;
-  const V6* base = a.is_rows + size_t(c) * a.is_stride;
+  const int total = n_sets * per_set;
+  const bool wit = wsrc.dst != nullptr;
   int wmin = kN + 1;
-  // The witness pass records the first codeword lighter than wthr.
-  const bool wit = a.witness != nullptr;
-  const int wthr = kN - d.tmax;
   for (int u = lane; u < total; u += 32) {
     const int j = u / per_set;
     int r = u - j * per_set;
     const V6* rows = base + size_t(j) * k * kIsVecPerRow;
+    const WitOut wo{wsrc.piv + j, wsrc.dst, wsrc.lock};
     if (r < n1) {
-      const V6 P = v6_ldg(rows + r * kIsVecPerRow);
+      const V6 P = v6_load<kCG>(rows + r * kIsVecPerRow);
       const int wt = __popc(lop3<0xFE>(P.l0, P.l1, P.l2)) + __popc(lop3<0xFE>(P.h0, P.h1, P.h2));
-      if (wit && wt < wthr) is_put_witness(wit_out(a, c, j), P.l0, P.l1, P.l2, P.h0, P.h1, P.h2);
+      if (wit && wt < wthr) is_put_witness(wo, P.l0, P.l1, P.l2, P.h0, P.h1, P.h2);
       wmin = min(wmin, wt);
       continue;
     }
@@ -1133,25 +1125,48 @@ __global__ void __launch_bounds__(128) levels123_kernel(DistArgs a) {
     int p = 1;  // pair q < p: C(p, 2) <= r < C(p + 1, 2)
     while ((p + 1) * p / 2 <= r) ++p;
     const int q = r - p * (p - 1) / 2;
-    const V6 Q = v6_ldg(rows + q * kIsVecPerRow);
+    const V6 Q = v6_load<kCG>(rows + q * kIsVecPerRow);
     if (t < 0) {
-      wmin = wit ? is_sweep_exact_w(Q, rows + p * kIsVecPerRow, wmin, wit_out(a, c, j), wthr)
-                 : is_sweep_exact<false>(Q, rows + p * kIsVecPerRow, wmin);
+      wmin = wit ? is_sweep_exact_w(Q, rows + p * kIsVecPerRow, wmin, wo, wthr)
+                 : is_sweep_exact<kCG>(Q, rows + p * kIsVecPerRow, wmin);
     } else {
-      V6 X = v6_ldg(rows + p * kIsVecPerRow);  // alpha^s row_p, s = 0..6
+      V6 X = v6_load<kCG>(rows + p * kIsVecPerRow);  // alpha^s row_p, s = 0..6
       for (int s7 = 0; s7 < 7; ++s7) {
         V6 P = Q;
         v6_xor(P, X);
-        wmin = wit ? is_sweep_exact_w(P, rows + t * kIsVecPerRow, wmin, wit_out(a, c, j), wthr)
-                   : is_sweep_exact<false>(P, rows + t * kIsVecPerRow, wmin);
+        wmin = wit ? is_sweep_exact_w(P, rows + t * kIsVecPerRow, wmin, wo, wthr)
+                   : is_sweep_exact<kCG>(P, rows + t * kIsVecPerRow, wmin);
         v6_alpha_pow(X, 1);
       }
     }
   }
   for (int o = 16; o > 0; o >>= 1) wmin = min(wmin, __shfl_xor_sync(0xffffffffu, wmin, o));
+  ncw = static_cast<unsigned long long>(n_sets) *
+        static_cast<unsigned long long>(n1 + 7 * n2 + 49 * n3);
+  return wmin;
+}
+
+// Levels 1 to 3 of every set of a batch in one launch, one warp per set.
+// These levels are too small to fill the GPU one launch each, and running
+// them without the bound check between them only adds codewords (the best
+// weight stays that of a codeword); level 4 onwards then follows the plan /
+// scan / walk triple.
+__global__ void __launch_bounds__(128) levels123_kernel(DistArgs a) {
+  const int lane = threadIdx.x & 31;
+  const int c = blockIdx.x * 4 + (threadIdx.x >> 5);
+  if (c >= a.n) return;  // warp-uniform
+  const CodeDesc d = a.desc[c];
+  if ((d.flags & kIsCodeFlag) == 0 || (d.flags & kDecidedFlag) != 0 || ld_flag(a.abort + c) != 0)
+    return;
+  // The witness pass records the first codeword lighter than the target.
+  const WitSrc wsrc = a.witness ? WitSrc{a.is_piv + size_t(c) * kIsMaxSets,
+                                         a.witness + size_t(c) * kN, a.wit_lock + c}
+                                : WitSrc{nullptr, nullptr, nullptr};
+  unsigned long long ncw = 0ull;
+  const int wmin = is_levels123_sets<false>(lane, a.is_rows + size_t(c) * a.is_stride, d.H, d.k,
+                                            wsrc, kN - d.tmax, ncw);
   if (lane == 0) {
-    atomicAdd(&a.is_hdr->codewords, static_cast<unsigned long long>(d.H) *
-                                        static_cast<unsigned long long>(n1 + 7 * n2 + 49 * n3));
+    atomicAdd(&a.is_hdr->codewords, ncw);
     if (wmin < a.is_best[c]) a.is_best[c] = wmin;
     if (a.is_best[c] < kN - d.tmax) a.abort[c] = 1;  // a witness below the target distance
   }

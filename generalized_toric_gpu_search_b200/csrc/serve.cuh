@@ -7,8 +7,9 @@
 //   SrvInput    one per slot: the request as submitted
 //   SrvResult   one per slot: the answer; `seq` = id + 1 is written last
 // Device arena:
-//   SrvDevHeader, S slots (request state, basis, pattern table), and the
-//   canonical dedup table (keys, values).
+//   SrvDevHeader; S slots (request state and its information set: k rows of
+//   g and six Gray deltas); the job ring; the canonical dedup table (keys,
+//   values).
 #pragma once
 
 #include "common.cuh"
@@ -17,11 +18,18 @@ namespace tg {
 
 constexpr int kSrvMaxK = kMaxExactK;
 constexpr int kSrvTPB = 128;
+constexpr int kSrvPerSm = 5;  // CTAs per SM: the walk's register and shared-memory budget
 
 enum : unsigned int { kSlotFree = 0, kSlotPrep = 1, kSlotRun = 2, kSlotWait = 3, kSlotDone = 4 };
 
 // Dedup table value: state << 56 | max_zeros << 48 | leader id.
 enum : unsigned int { kEntEmpty = 0, kEntInFlight = 1, kEntExact = 2, kEntAbort = 3 };
+
+// Claim word of a request: id << 32 | level << 27 | next unclaimed task of
+// that level.  Done word: level << 40 | tasks of that level counted.
+constexpr unsigned long long kSrvTaskMask = (1ull << 27) - 1ull;
+constexpr unsigned long long kSrvMaxTasks = (1ull << 27) - (1ull << 20);
+constexpr unsigned long long kSrvDoneMask = (1ull << 40) - 1ull;
 
 struct SrvCtl {
   unsigned int published;  // requests 0..published-1 are in pubq/inputs
@@ -48,33 +56,33 @@ struct SrvResult {
 
 struct SrvDevHeader {
   unsigned int prep_next;             // next published request to prepare
-  unsigned int lo;                    // oldest request that may still need a warp
+  unsigned int pub_mirror;            // device copy of SrvCtl::published
   unsigned long long last_activity;   // globaltimer of the last useful step
   int status;
   unsigned int launches;
+  unsigned int job_head;              // next job to serve
+  unsigned int job_tail;              // next free job position
+  unsigned int stop_mirror;           // device copy of SrvCtl::stop
+  unsigned int pad0;
   unsigned long long tasks_done;
-  unsigned long long codewords;
+  unsigned long long codewords;       // codewords evaluated (levels 1-3 and the level tasks)
   unsigned long long dedup_hits;
   unsigned long long finished;
-  unsigned int trace_n;                 // lo advances recorded so far
-  unsigned int pub_mirror;              // device copy of SrvCtl::published
-  unsigned long long trace[32][4];      // last lo advances: i|reason, id|state, n_tasks, claim
-  unsigned int stop_mirror;             // device copy of SrvCtl::stop
-  unsigned int pad1;
-  unsigned long long scan_steps;        // request entries looked at by scanners
-  unsigned long long host_reads;        // refreshes of the mirrors from host memory
+  unsigned long long levels_opened;   // level jobs pushed
+  unsigned long long wait_requeues;   // wait jobs put back behind the others
+  unsigned long long host_reads;      // refreshes of the mirrors from host memory
 };
 
 struct SrvSlotHdr {
   unsigned int state;
   unsigned int id;
-  int k, R, H, n_pat, tmax;
-  int best;
-  int abort;
+  int k, tmax;
+  int best;    // smallest weight met (levels done and tasks counted); 64 = none
+  int abort;   // a weight below the target distance was met
   int leader;
-  unsigned long long n_tasks;     // < 2^31
-  unsigned long long claim;       // id << 32 | next unclaimed task (generation-tagged)
-  unsigned long long done_tasks;
+  int level;   // level whose tasks are out
+  unsigned long long claim;
+  unsigned long long done;
   unsigned long long tslot;  // dedup table slot or ~0
   unsigned long long t_admit;
   int idx[24];
@@ -88,15 +96,16 @@ struct SrvArgs {
   SrvDevHeader* dh;
   uint8_t* slots;
   size_t slot_bytes;
-  size_t basis_off, cum_off, info_off;
-  unsigned long long* ring;   // device copy of pubq, written by each request's preparer
+  size_t rows_off;            // the information set within a slot
+  unsigned long long* jobs;   // job ring: id << 32 | level << 24 | slot (0 = empty)
+  unsigned int J;             // job ring capacity (power of two)
   unsigned long long* keys;
   unsigned long long* vals;
   unsigned long long table_cap;
   int S;
   int Q;
   int k_max;
-  int R;
+  int lanes;                  // resident threads of the loop (task sizing)
   unsigned long long idle_ns;
   unsigned long long life_ns;
   DeviceTables tab;

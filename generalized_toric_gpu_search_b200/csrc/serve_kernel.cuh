@@ -1,19 +1,23 @@
 // Serving-loop kernel.  Included at the end of distance.cu, whose GF(8)
-// constant tables and prep / walk device functions it shares.
+// tables and information-set device code it shares.
 //
-// Every warp of a persistent grid loops:
-//   1. prepare the next published request, if any: read it from host-mapped
-//      memory, compute its AGL2(F7) canonical mask, look it up in the device
-//      dedup table (answer at once from an equivalent finished request when
-//      that answer is conclusive for this request's threshold, wait for an
-//      equivalent request in flight, else evaluate), build its basis and task
-//      table and mark it runnable;
-//   2. otherwise claim 32 tasks of the oldest runnable request (one per lane),
-//      walk them, and finalise the request when its last task is counted;
-//   3. otherwise resolve a waiting request whose equivalent has finished;
-//   4. otherwise sleep briefly; leave when nothing happened for idle_ns.
-// Requests published while others run are prepared and their tasks join the
-// same pool, so their work overlaps on the device (continuous batching).
+// A request is evaluated by information sets, level by level, like a code of
+// a batch (infoset_kernel.cuh): its preparing warp computes its canonical
+// mask and looks it up in the dedup table, then eliminates its k rows to one
+// information set, walks levels 1 to 3 itself and, while the torus-orbit
+// bound ceil(49 (L + 1) / k) stays below its best weight, opens level 4.
+// Every level of every request is a job in one device ring; warps take 32
+// tasks at a time from the oldest job, so the levels of requests admitted at
+// different times share the SMs (continuous batching).  The warp that counts
+// a level's last task settles the request or opens its next level.
+//
+// Every warp of the persistent grid loops:
+//   1. prepare the next published request, if any;
+//   2. otherwise serve the job at the head of the ring: claim 32 tasks of
+//      its level, or, for a request waiting on an equivalent one still in
+//      flight, resolve it once that one's answer is final (else requeue it);
+//      a job with nothing left to claim is popped;
+//   3. otherwise sleep briefly; leave when nothing happened for idle_ns.
 // All waits are bounded: the loop exits on the host's stop flag, after
 // life_ns, or after idle_ns without work; the host relaunches it while
 // requests are outstanding.  No warp ever waits for another warp.
@@ -59,6 +63,10 @@ __device__ __forceinline__ SrvSlotHdr* srv_slot(const SrvArgs& a, unsigned int s
   return reinterpret_cast<SrvSlotHdr*>(a.slots + size_t(slot) * a.slot_bytes);
 }
 
+__device__ __forceinline__ V6* srv_rows(const SrvArgs& a, SrvSlotHdr* h) {
+  return reinterpret_cast<V6*>(reinterpret_cast<uint8_t*>(h) + a.rows_off);
+}
+
 __device__ __forceinline__ unsigned long long ent_pack(unsigned int st, int mz, unsigned int id) {
   return (static_cast<unsigned long long>(st) << 56) |
          (static_cast<unsigned long long>(mz & 0xFF) << 48) | id;
@@ -68,6 +76,44 @@ __device__ __forceinline__ unsigned long long ent_pack(unsigned int st, int mz, 
 // GL2 point table read through L1 (the anchored minimum of canonical.cu).
 __device__ uint64_t canon_mask_warp(int lane, uint64_t S, const uint8_t* gl2) {
   return canon_mask_warp_min<true>(lane, S, gl2);
+}
+
+// Units of level w of a k-row request (one information set).
+__device__ __forceinline__ unsigned long long srv_units(const unsigned long long (*bn)[kIsBinom],
+                                                       int k, int w) {
+  return bn[k][w] * is_units_per_support(w);
+}
+
+// Units per task of a level: the batch scan's rule for one code (about eight
+// tasks per resident thread, at most 343 units, aligned with supports), grown
+// by factors of 7 until the level has fewer than kSrvMaxTasks tasks (the claim
+// word's task field).
+__device__ __forceinline__ unsigned long long srv_task_units(unsigned long long units, int w,
+                                                            int lanes) {
+  const unsigned long long target = 8ull * static_cast<unsigned long long>(lanes);
+  unsigned long long nb = (units + target - 1ull) / target;
+  nb = max(1ull, min(nb, 343ull));
+  const unsigned long long bps = is_units_per_support(w);
+  if (bps > 1ull) {
+    if (nb >= bps) {
+      nb = (nb / bps) * bps;
+    } else {
+      unsigned long long p7 = 1ull;
+      while (p7 * 7ull <= nb) p7 *= 7ull;
+      nb = (nb * nb > 7ull * p7 * p7) ? 7ull * p7 : p7;
+    }
+  }
+  while ((units + nb - 1ull) / nb >= kSrvMaxTasks) nb *= 7ull;
+  return nb;
+}
+
+// Appends a job: level w >= 4 of request gen in `slot`, or (w = 0) the
+// request waiting there on an equivalent one.
+__device__ void srv_push_job(const SrvArgs& a, unsigned int gen, int w, unsigned int slot) {
+  const unsigned int pos = atomicAdd(&a.dh->job_tail, 1u);
+  const unsigned long long e = (static_cast<unsigned long long>(gen) << 32) |
+                               (static_cast<unsigned long long>(w) << 24) | slot;
+  atomicExch(a.jobs + (pos & (a.J - 1u)), e);
 }
 
 // Writes the final answer of a request to host-mapped memory and frees the
@@ -90,57 +136,103 @@ __device__ void srv_finish(const SrvArgs& a, unsigned int slot, SrvSlotHdr* h, i
   *reinterpret_cast<volatile unsigned int*>(&r->seq) = id + 1u;
 }
 
-// Settles a request with its final value: records it in the dedup table
-// (leaders always; other requests when the value is exact) and writes the
-// answer.  `aborted` means the value is only a witness above the threshold.
+// Settles a request with max_zeros m: records it in the dedup table (leaders
+// always; other requests when the value is exact) and writes the answer.
+// `witness` means m is only a witness above the threshold.
 __device__ void srv_settle(const SrvArgs& a, unsigned int slot, SrvSlotHdr* h, int m,
-                           bool aborted) {
+                           bool witness) {
   const unsigned long long ts = __ldcg(&h->tslot);
-  if (ts != ~0ull && (__ldcg(&h->leader) || !aborted)) {
-    atomicExch(a.vals + ts, ent_pack(aborted ? kEntAbort : kEntExact, m, __ldcg(&h->id)));
+  if (ts != ~0ull && (__ldcg(&h->leader) || !witness)) {
+    __threadfence();
+    atomicExch(a.vals + ts, ent_pack(witness ? kEntAbort : kEntExact, m, __ldcg(&h->id)));
   }
   const int tmax = __ldcg(&h->tmax);
-  srv_finish(a, slot, h, m, (aborted || m > tmax) ? TG_RESULT_FAIL : TG_RESULT_PASS);
+  srv_finish(a, slot, h, m, (witness || m > tmax) ? TG_RESULT_FAIL : TG_RESULT_PASS);
 }
 
-// Finalises an evaluated request once all its tasks are counted.
-__device__ void srv_complete(const SrvArgs& a, unsigned int slot, SrvSlotHdr* h) {
+// Opens level w of request gen: its done count, then its claim word (from
+// here on a claim tagged (gen, w) refers to this level), then its job.
+__device__ void srv_open_level(const SrvArgs& a, unsigned int slot, SrvSlotHdr* h,
+                               unsigned int gen, int w) {
+  atomicExch(&h->done, static_cast<unsigned long long>(w) << 40);
+  h->level = w;
   __threadfence();
-  const int m = atomicAdd(&h->best, 0);
-  const bool aborted = atomicAdd(&h->abort, 0) != 0;
-  srv_settle(a, slot, h, m, aborted);
+  atomicExch(&h->claim, (static_cast<unsigned long long>(gen) << 32) |
+                            (static_cast<unsigned long long>(w) << 27));
+  __threadfence();
+  srv_push_job(a, gen, w, slot);
+  atomicAdd(&a.dh->levels_opened, 1ull);
 }
 
-// Builds the walk of a request whose indices are in h->idx (warp-level).
-__device__ void srv_evaluate(const SrvArgs& a, int lane, unsigned int slot, SrvSlotHdr* h,
-                             int* s_idx, int* s_row) {
+// After levels 1..w of a request: settle it (a witness below the target,
+// the bound met, or every level done) or open level w + 1.  One thread.
+__device__ void srv_level_end(const SrvArgs& a, unsigned int slot, SrvSlotHdr* h,
+                              unsigned int gen, int w) {
+  __threadfence();
+  const int best = atomicAdd(&h->best, 0);
   const int k = __ldcg(&h->k);
-  s_idx[lane] = lane < k ? __ldcg(&h->idx[lane]) : -1;
+  const int tmax = __ldcg(&h->tmax);
+  if (atomicAdd(&h->abort, 0) != 0 || best < kN - tmax) {
+    srv_settle(a, slot, h, kN - best, true);
+    return;
+  }
+  const int bound = (kN * (w + 1) + k - 1) / k;
+  if (w >= k || best <= bound) {
+    srv_settle(a, slot, h, kN - best, false);
+    return;
+  }
+  srv_open_level(a, slot, h, gen, w + 1);
+}
+
+// Evaluates a request whose indices are in h->idx (warp-level): one
+// information set by Gauss-Jordan elimination, levels 1 to 3 by this warp,
+// then level 4 as a job unless the request is decided.
+__device__ void srv_evaluate(const SrvArgs& a, int lane, unsigned int slot, SrvSlotHdr* h,
+                             uint8_t* s_ord) {
+  const int k = __ldcg(&h->k);
+  const unsigned int gen = __ldcg(&h->id);
+  const int tmax = __ldcg(&h->tmax);
+  if (k == 0) {
+    if (lane == 0) srv_settle(a, slot, h, 0, false);
+    return;
+  }
+  const int my = lane < k ? __ldcg(&h->idx[lane]) : 0;
+  uint64_t p0 = 0ull, p1 = 0ull, p2 = 0ull;
+  if (lane < k) {
+    for (int j = 0; j < kN; ++j) {
+      const uint64_t v = a.tab.M[my * kN + j];
+      p0 |= (v & 1ull) << j;
+      p1 |= ((v >> 1) & 1ull) << j;
+      p2 |= ((v >> 2) & 1ull) << j;
+    }
+  }
+  is_make_order(s_ord, 0, lane);
+  uint64_t used = 0ull;
+  if (is_gauss_jordan(lane, k, p0, p1, p2, used, s_ord) < k) {
+    // dependent rows: a nonzero message gives the zero codeword
+    if (lane == 0) srv_settle(a, slot, h, kN, false);
+    return;
+  }
+  is_reorder_columns(used, p0, p1, p2);
+  V6* rows = srv_rows(a, h);
+  is_store_set(rows, lane, k, p0, p1, p2);
+  __threadfence_block();
   __syncwarp();
-  uint8_t* base = reinterpret_cast<uint8_t*>(h);
-  V6* B = reinterpret_cast<V6*>(base + a.basis_off);
-  uint64_t* cum = reinterpret_cast<uint64_t*>(base + a.cum_off);
-  uint32_t* info = reinterpret_cast<uint32_t*>(base + a.info_off);
-  const PrepResult pr = prep_code(lane, k, s_idx, s_row, a.R, TG_ENUM_ORBIT,
-                                  TG_VARIANT_HISTOGRAM, a.tab.M, B, cum, info);
+  unsigned long long ncw = 0ull;
+  const int wmin = is_levels123_sets<true>(lane, rows, 1, k, WitSrc{nullptr, nullptr, nullptr},
+                                           kN - tmax, ncw);
   if (lane == 0) {
-    if (pr.n_tasks == 0) {
-      srv_settle(a, slot, h, pr.result, false);  // decided exactly without a walk
+    atomicAdd(&a.dh->codewords, ncw);
+    h->best = wmin;
+    h->abort = 0;
+    if (wmin < kN - tmax) {
+      srv_settle(a, slot, h, kN - wmin, true);
+    } else if (k <= 3 || wmin <= (kN * 4 + k - 1) / k) {
+      srv_settle(a, slot, h, kN - wmin, false);
     } else {
-      h->R = pr.R;
-      h->H = pr.H;
-      h->n_pat = pr.n_pat;
-      h->best = 0;
-      h->abort = 0;
-      h->done_tasks = 0ull;
-      h->n_tasks = pr.n_tasks;
-      atomicAdd(&a.dh->codewords, static_cast<unsigned long long>(pr.n_tasks * pow8(pr.R)));
-      __threadfence();
-      // From here on a claim tagged with this request's id refers to the
-      // tables written above, whatever the claimer believed about the slot.
-      atomicExch(&h->claim, static_cast<unsigned long long>(__ldcg(&h->id)) << 32);
       __threadfence();
       *reinterpret_cast<volatile unsigned int*>(&h->state) = kSlotRun;
+      srv_open_level(a, slot, h, gen, 4);
     }
   }
   __syncwarp();
@@ -167,8 +259,7 @@ __device__ bool srv_from_entry(const SrvArgs& a, unsigned int slot, SrvSlotHdr* 
 }
 
 // Prepares published request `req` (warp-level).
-__device__ void srv_prepare(const SrvArgs& a, int lane, unsigned int req, int* s_idx,
-                            int* s_row) {
+__device__ void srv_prepare(const SrvArgs& a, int lane, unsigned int req, uint8_t* s_ord) {
   unsigned long long e = 0ull;
   if (lane == 0) {
     // pubq[req] was written before `published` moved past req; reread a
@@ -188,7 +279,6 @@ __device__ void srv_prepare(const SrvArgs& a, int lane, unsigned int req, int* s
   SrvSlotHdr* h = srv_slot(a, slot);
   const SrvInput* in = a.inputs + slot;
   if (lane == 0) {
-    *reinterpret_cast<volatile unsigned long long*>(a.ring + (req % unsigned(a.Q))) = e;
     *reinterpret_cast<volatile unsigned int*>(&h->state) = kSlotPrep;
     __threadfence();
     *reinterpret_cast<volatile unsigned int*>(&h->id) = req;
@@ -206,6 +296,7 @@ __device__ void srv_prepare(const SrvArgs& a, int lane, unsigned int req, int* s
     h->tmax = kN - td;
     h->tslot = ~0ull;
     h->leader = 0;
+    h->level = 0;
   }
   if (lane < 24) h->idx[lane] = (!bad_k && lane < k) ? my : 0;
   __syncwarp();
@@ -247,8 +338,10 @@ __device__ void srv_prepare(const SrvArgs& a, int lane, unsigned int req, int* s
       if (lane == 0) {
         const unsigned int st = static_cast<unsigned int>(v >> 56);
         if (st == kEntEmpty || st == kEntInFlight) {
+          // the equivalent request is still running: wait in the job ring
           __threadfence();
           *reinterpret_cast<volatile unsigned int*>(&h->state) = kSlotWait;
+          srv_push_job(a, req, 0, slot);
           done = true;
         } else {
           done = srv_from_entry(a, slot, h, v);
@@ -258,70 +351,87 @@ __device__ void srv_prepare(const SrvArgs& a, int lane, unsigned int req, int* s
       if (done) return;
     }
   }
-  srv_evaluate(a, lane, slot, h, s_idx, s_row);
+  srv_evaluate(a, lane, slot, h, s_ord);
 }
 
-// Resolves a waiting request (its state was moved WAIT -> PREP by lane 0).
-__device__ void srv_resolve(const SrvArgs& a, int lane, unsigned int slot, int* s_idx,
-                            int* s_row) {
+// Resolves a waiting request whose equivalent has an answer (warp-level):
+// from that answer when conclusive, else by its own evaluation.
+__device__ void srv_resolve(const SrvArgs& a, int lane, unsigned int slot, uint8_t* s_ord) {
   SrvSlotHdr* h = srv_slot(a, slot);
   bool done = false;
   if (lane == 0) done = srv_from_entry(a, slot, h, ld_vol64(a.vals + __ldcg(&h->tslot)));
   done = __shfl_sync(0xffffffffu, done, 0);
-  if (!done) srv_evaluate(a, lane, slot, h, s_idx, s_row);
+  if (!done) srv_evaluate(a, lane, slot, h, s_ord);
 }
 
-// Runs tasks c0 .. c0+31 of request `gen` in `slot`, one per lane.  The claim
-// was taken on the generation-tagged counter, so `gen` is the request whose
-// tables the slot holds; a claim on a generation the slot no longer serves is
-// dropped (that request has finished, so no task of it was left unclaimed).
-__device__ void srv_run(const SrvArgs& a, int lane, unsigned int slot, unsigned int gen,
-                        unsigned long long c0) {
+// Runs the 32 tasks a warp claimed: `cw` is the claim word's value before
+// the warp's atomicAdd (request gen, level w, first task t0).  A claim on a
+// slot that no longer serves gen, or past the level's end, runs nothing.
+// The warp that counts a level's last task ends the level.
+__device__ void srv_run(const SrvArgs& a, int lane, unsigned int slot, unsigned long long cw,
+                        const unsigned long long (*bn)[kIsBinom], uint16_t* dig, uint32_t* ez) {
   SrvSlotHdr* h = srv_slot(a, slot);
-  if (ld_vol32(&h->id) != gen) return;
+  const unsigned int gen = static_cast<unsigned int>(cw >> 32);
+  const int w = static_cast<int>((cw >> 27) & 31ull);
+  const unsigned long long t0 = cw & kSrvTaskMask;
+  if (ld_vol32(&h->id) != gen || w < 4) return;
   __threadfence();
-  const unsigned long long n_tasks = __ldcg(&h->n_tasks);
-  if (c0 >= n_tasks) return;
-  const unsigned long long t = c0 + unsigned(lane);
-  const uint8_t* base = reinterpret_cast<const uint8_t*>(h);
-  const V6* B = reinterpret_cast<const V6*>(base + a.basis_off);
-  const uint64_t* cum = reinterpret_cast<const uint64_t*>(base + a.cum_off);
-  const uint32_t* info = reinterpret_cast<const uint32_t*>(base + a.info_off);
-  bool last = false;
-  if (t < n_tasks && !ld_flag(&h->abort)) {
-    const int p = last_le<true>(cum, __ldcg(&h->n_pat), t);
-    const uint64_t q = t - ld_u64<true>(cum + p);
-    bool aborted = false;
-    const int m = hist_task<true>(B, ld_u32<true>(info + p), q, __ldcg(&h->H), __ldcg(&h->k),
-                                  __ldcg(&h->R), __ldcg(&h->tmax), &h->abort, aborted);
-    if (m > 0) atomicMax(&h->best, m);
-    if (aborted) {
-      atomicExch(&h->abort, 1);
-      const unsigned long long tag = static_cast<unsigned long long>(gen) << 32;
-      const unsigned long long old = atomicMax(&h->claim, tag | n_tasks);
-      const unsigned long long old_next = old & 0xFFFFFFFFull;
-      if ((old >> 32) == gen && old_next < n_tasks) {
-        __threadfence();
-        const unsigned long long skipped = n_tasks - old_next;
-        if (atomicAdd(&h->done_tasks, skipped) + skipped == n_tasks) last = true;
+  const int k = __ldcg(&h->k);
+  const int tmax = __ldcg(&h->tmax);
+  const unsigned long long units = srv_units(bn, k, w);
+  const unsigned long long nb = srv_task_units(units, w, a.lanes);
+  const unsigned long long nt = (units + nb - 1ull) / nb;
+  if (t0 >= nt) return;
+  const int wthr = kN - tmax;
+  const unsigned long long t = t0 + unsigned(lane);
+  int wmin = kN + 1;
+  unsigned long long ncw = 0ull;
+  if (t < nt && !ld_flag(&h->abort)) {
+    const unsigned long long u0 = t * nb;
+    const unsigned long long u1 = min(u0 + nb, units);
+    wmin = is_walk_range<kSrvTPB, false, true>(srv_rows(a, h), 1, 0, &h->abort,
+                                               WitSrc{nullptr, nullptr, nullptr}, bn, dig, ez,
+                                               k, w, u0, u1, wthr, ld_flag(&h->best), ncw);
+  }
+  const int wl = __reduce_min_sync(0xffffffffu, wmin);
+  for (int o = 16; o > 0; o >>= 1) ncw += __shfl_xor_sync(0xffffffffu, ncw, o);
+  if (lane == 0) {
+    atomicAdd(&a.dh->codewords, ncw);
+    unsigned long long skipped = 0ull;
+    if (wl < ld_flag(&h->best)) {
+      const int best = min(atomicMin(&h->best, wl), wl);
+      if (best < wthr && atomicExch(&h->abort, 1) == 0) {
+        // a witness below the target: the level's unclaimed tasks are
+        // skipped, and counted here
+        const unsigned long long tag = cw & ~kSrvTaskMask;
+        const unsigned long long old = atomicMax(&h->claim, tag | nt);
+        if ((old & ~kSrvTaskMask) == tag && (old & kSrvTaskMask) < nt)
+          skipped = nt - (old & kSrvTaskMask);
       }
     }
+    const unsigned long long owned = min(32ull, nt - t0);
+    __threadfence();
+    const unsigned long long add = owned + skipped;
+    const unsigned long long old = atomicAdd(&h->done, add);
+    atomicAdd(&a.dh->tasks_done, owned);
+    if ((old >> 40) == static_cast<unsigned long long>(w) && (old & kSrvDoneMask) + add == nt)
+      srv_level_end(a, slot, h, gen, w);
   }
   __syncwarp();
-  const unsigned long long owned = min(32ull, n_tasks - c0);
-  if (lane == 0) {
-    __threadfence();
-    if (atomicAdd(&h->done_tasks, owned) + owned == n_tasks) last = true;
-    atomicAdd(&a.dh->tasks_done, owned);
-  }
-  if (last) srv_complete(a, slot, h);
 }
 
-__global__ void __launch_bounds__(kSrvTPB, 8) serve_kernel(SrvArgs a) {
-  __shared__ int s_idx[kSrvTPB / 32][32];
-  __shared__ int s_row[kSrvTPB / 32][32];
+__global__ void __launch_bounds__(kSrvTPB, kSrvPerSm) serve_kernel(SrvArgs a) {
+  __shared__ unsigned long long s_binom[kIsBinom][kIsBinom];
+  __shared__ uint16_t s_dig[kIsMaxDigits][kSrvTPB];
+  __shared__ uint32_t s_ez[39][kSrvTPB];
+  __shared__ uint8_t s_ord[kSrvTPB / 32][64];
+  for (int i = threadIdx.x; i < kIsBinom * kIsBinom; i += kSrvTPB)
+    s_binom[i / kIsBinom][i % kIsBinom] = c_binom[i / kIsBinom][i % kIsBinom];
+  __syncthreads();
   const int lane = threadIdx.x & 31;
-  const int w = threadIdx.x >> 5;
+  const int wl = threadIdx.x >> 5;
+  uint16_t* my_dig = &s_dig[0][threadIdx.x];
+  uint32_t* my_ez = &s_ez[0][threadIdx.x];
   const unsigned long long t_start = gtimer();
   if (threadIdx.x == 0 && blockIdx.x == 0) {
     atomicMax(&a.dh->last_activity, t_start);
@@ -332,7 +442,7 @@ __global__ void __launch_bounds__(kSrvTPB, 8) serve_kernel(SrvArgs a) {
   for (;;) {
     int action = 0;  // -1 exit, 0 idle, 1 prepare, 2 run, 3 resolve
     unsigned int arg = 0u, slot = 0u;
-    unsigned long long c0 = 0ull;
+    unsigned long long cw = 0ull;
     if (lane == 0) {
       // Host memory is read over the bus: only an idle warp, or every warp
       // once in 64 steps, refreshes the device mirrors of the host's counters.
@@ -342,7 +452,6 @@ __global__ void __launch_bounds__(kSrvTPB, 8) serve_kernel(SrvArgs a) {
         atomicAdd(&a.dh->host_reads, 1ull);
       }
       const unsigned long long now = gtimer();
-      unsigned int steps = 0u;
       if (ld_vol32(&a.dh->stop_mirror) || now - t_start > a.life_ns) {
         action = -1;
       } else {
@@ -357,81 +466,57 @@ __global__ void __launch_bounds__(kSrvTPB, 8) serve_kernel(SrvArgs a) {
           }
           p = prev;
         }
-        if (action == 0) {
-          unsigned int lo = ld_vol32(&a.dh->lo);
-          const unsigned int prepped = min(pub, ld_vol32(&a.dh->prep_next));
-          for (unsigned int i = lo, n = 0; i < prepped && n < unsigned(a.S) + 1u; ++i, ++n) {
-            ++steps;
-            const unsigned long long e = ld_vol64(a.ring + (i % unsigned(a.Q)));
-            const unsigned int eg = static_cast<unsigned int>(e >> 32);
-            bool finished = false;  // nothing left to claim or resolve at i
-            unsigned int why = 0u, t_hid = 0u, t_st = 0u;
-            unsigned long long t_nt = 0ull, t_cw = 0ull;
-            if (eg != i) {
-              // A later request owns the ring entry only once request i has
-              // been answered; anything else is an entry not yet visible.
-              finished = eg != 0xFFFFFFFFu && eg > i && (eg - i) % unsigned(a.Q) == 0u;
-              why = 1u;
-              t_cw = e;
+        // The job at the head of the ring: claim from it, or pop it.  A few
+        // tries per step keep the warp from looping on a busy ring.
+        for (int tries = 0; action == 0 && tries < 8; ++tries) {
+          const unsigned int hd = ld_vol32(&a.dh->job_head);
+          if (hd == ld_vol32(&a.dh->job_tail)) break;
+          unsigned long long* je = a.jobs + (hd & (a.J - 1u));
+          const unsigned long long e = ld_vol64(je);
+          if (e == 0ull) break;  // pushed but not yet written
+          const unsigned int gen = static_cast<unsigned int>(e >> 32);
+          const int w = static_cast<int>((e >> 24) & 0xFFull);
+          const unsigned int sl = static_cast<unsigned int>(e & 0xFFFFFFull);
+          SrvSlotHdr* h = srv_slot(a, sl);
+          if (w == 0) {
+            // a waiting request: take the job; resolve it once its
+            // equivalent's answer is final, else put it back behind the rest
+            if (atomicCAS(&a.dh->job_head, hd, hd + 1u) != hd) continue;
+            atomicExch(je, 0ull);
+            if (ld_vol32(&h->id) != gen || ld_vol32(&h->state) != kSlotWait) continue;
+            const unsigned long long v = ld_vol64(a.vals + __ldcg(&h->tslot));
+            if ((v >> 56) >= kEntExact &&
+                atomicCAS(&h->state, kSlotWait, kSlotPrep) == kSlotWait) {
+              action = 3;
+              slot = sl;
             } else {
-              const unsigned int sl = static_cast<unsigned int>(e);
-              SrvSlotHdr* h = srv_slot(a, sl);
-              const unsigned int hid = ld_vol32(&h->id);
-              t_hid = hid;
-              if (hid > i) {
-                finished = true;  // the slot already serves a newer request
-                why = 2u;
-              } else if (hid == i) {
-                __threadfence();
-                const unsigned int st = ld_vol32(&h->state);
-                __threadfence();  // n_tasks after state: RUN publishes it
-                const unsigned long long nt = __ldcg(&h->n_tasks);
-                if (st == kSlotRun) {
-                  const unsigned long long cw = ld_vol64(&h->claim);
-                  if ((cw >> 32) == i && (cw & 0xFFFFFFFFull) < nt) {
-                    const unsigned long long old = atomicAdd(&h->claim, 32ull);
-                    c0 = old & 0xFFFFFFFFull;
-                    arg = static_cast<unsigned int>(old >> 32);
-                    if (arg != i || c0 < nt) {  // a task of generation arg, or past i's end
-                      action = 2;
-                      slot = sl;
-                      break;
-                    }
-                  }
-                  if ((cw >> 32) == i) finished = true;
-                  why = 3u;
-                  t_st = st;
-                  t_nt = nt;
-                  t_cw = cw;
-                } else if (st == kSlotWait) {
-                  const unsigned long long v = ld_vol64(a.vals + __ldcg(&h->tslot));
-                  if ((v >> 56) >= kEntExact &&
-                      atomicCAS(&h->state, kSlotWait, kSlotPrep) == kSlotWait) {
-                    action = 3;
-                    slot = sl;
-                    break;
-                  }
-                } else if (st == kSlotDone) {
-                  finished = true;
-                  why = 4u;
-                  t_st = st;
-                }
-              }
+              srv_push_job(a, gen, 0, sl);
+              atomicAdd(&a.dh->wait_requeues, 1ull);
             }
-            if (finished && i == lo) {
-              if (atomicCAS(&a.dh->lo, lo, lo + 1u) == lo) {
-                const unsigned int tn = atomicAdd(&a.dh->trace_n, 1u) & 31u;
-                a.dh->trace[tn][0] = (static_cast<unsigned long long>(i) << 8) | why;
-                a.dh->trace[tn][1] = (static_cast<unsigned long long>(t_hid) << 8) | t_st;
-                a.dh->trace[tn][2] = t_nt;
-                a.dh->trace[tn][3] = t_cw;
-              }
-              lo = ld_vol32(&a.dh->lo);
-              if (lo > i + 1u) { i = lo - 1u; }
-            }
+            continue;
+          }
+          const unsigned long long tag = (static_cast<unsigned long long>(gen) << 32) |
+                                         (static_cast<unsigned long long>(w) << 27);
+          const unsigned long long cur = ld_vol64(&h->claim);
+          bool open = false;
+          if ((cur & ~kSrvTaskMask) == tag) {
+            const int k = __ldcg(&h->k);
+            const unsigned long long units = srv_units(s_binom, k, w);
+            const unsigned long long nt =
+                (units + srv_task_units(units, w, a.lanes) - 1ull) /
+                srv_task_units(units, w, a.lanes);
+            open = (cur & kSrvTaskMask) < nt;
+          }
+          if (open) {
+            // whatever the claim returns is this warp's to run (srv_run
+            // checks the request and the level's end)
+            cw = atomicAdd(&h->claim, 32ull);
+            action = 2;
+            slot = sl;
+          } else if (atomicCAS(&a.dh->job_head, hd, hd + 1u) == hd) {
+            atomicExch(je, 0ull);
           }
         }
-        if (steps) atomicAdd(&a.dh->scan_steps, static_cast<unsigned long long>(steps));
         if (action == 0) {
           const unsigned long long act = max(ld_vol64(&a.dh->last_activity), t_start);
           if (now > act + a.idle_ns) action = -1;
@@ -447,12 +532,12 @@ __global__ void __launch_bounds__(kSrvTPB, 8) serve_kernel(SrvArgs a) {
     }
     arg = __shfl_sync(0xffffffffu, arg, 0);
     slot = __shfl_sync(0xffffffffu, slot, 0);
-    c0 = __shfl_sync(0xffffffffu, c0, 0);
+    cw = __shfl_sync(0xffffffffu, cw, 0);
     __syncwarp();  // order every lane's loads after lane 0's acquire
     if (lane == 0) atomicMax(&a.dh->last_activity, gtimer());
-    if (action == 1) srv_prepare(a, lane, arg, s_idx[w], s_row[w]);
-    else if (action == 2) srv_run(a, lane, slot, arg, c0);
-    else srv_resolve(a, lane, slot, s_idx[w], s_row[w]);
+    if (action == 1) srv_prepare(a, lane, arg, s_ord[wl]);
+    else if (action == 2) srv_run(a, lane, slot, cw, s_binom, my_dig, my_ez);
+    else srv_resolve(a, lane, slot, s_ord[wl]);
     if (lane == 0) atomicMax(&a.dh->last_activity, gtimer());
   }
 }

@@ -20,9 +20,10 @@ namespace tg {
 static size_t a256(size_t x) { return (x + 255) & ~size_t(255); }
 
 struct SrvLayout {
-  int S, Q, R, k_max, P;
-  size_t slot_bytes, basis_off, cum_off, info_off;
-  size_t d_hdr, d_slots, d_ring, d_keys, d_vals, d_total;
+  int S, Q, k_max;
+  unsigned int J;
+  size_t slot_bytes, rows_off;
+  size_t d_hdr, d_slots, d_jobs, d_keys, d_vals, d_total;
   size_t h_ctl, h_pubq, h_inputs, h_results, h_total;
   unsigned long long table_cap;
 };
@@ -33,19 +34,13 @@ static int srv_defaults(const tg_server_params* p, tg_server_params& q) {
     set_last_error("server k_max must be 1..%d", kSrvMaxK);
     return TG_ERR_INVALID_ARGUMENT;
   }
-  if (q.tail_rows == 0) q.tail_rows = 4;
-  if (q.tail_rows < 2 || q.tail_rows > 7) {
-    set_last_error("server tail_rows must be 0 or 2..7");
+  if (q.tail_rows != 0 && (q.tail_rows < 2 || q.tail_rows > 7)) {
+    set_last_error("server tail_rows must be 0 or 2..7 (it is not used by the loop)");
     return TG_ERR_INVALID_ARGUMENT;
   }
-  if (q.k_max - q.tail_rows > 12) {
-    // keeps every request's task count below 2^31 (the claim word's 32 bits)
-    set_last_error("server k_max - tail_rows must be <= 12");
-    return TG_ERR_INVALID_ARGUMENT;
-  }
-  if (q.blocks_per_sm == 0) q.blocks_per_sm = 8;
-  if (q.blocks_per_sm < 1 || q.blocks_per_sm > 8) {
-    set_last_error("server blocks_per_sm must be 0..8");
+  if (q.blocks_per_sm == 0) q.blocks_per_sm = kSrvPerSm;
+  if (q.blocks_per_sm < 1 || q.blocks_per_sm > kSrvPerSm) {
+    set_last_error("server blocks_per_sm must be 0..%d", kSrvPerSm);
     return TG_ERR_INVALID_ARGUMENT;
   }
   if (q.idle_us == 0) q.idle_us = 2000;
@@ -68,22 +63,29 @@ static int srv_defaults(const tg_server_params* p, tg_server_params& q) {
   return TG_OK;
 }
 
+// Job ring capacity: a power of two above every job a full pool of requests
+// can have pushed and not yet popped (each request pushes at most one job
+// per level, k - 3 <= 18 levels, plus wait jobs that replace one another).
+static unsigned int srv_job_capacity(int S) {
+  unsigned long long need = 32ull * static_cast<unsigned long long>(S) + 1024ull;
+  unsigned long long J = 1024ull;
+  while (J < need) J <<= 1;
+  return static_cast<unsigned int>(J);
+}
+
 static SrvLayout srv_layout(const tg_server_params& q, int S) {
   SrvLayout L{};
   L.S = S;
   L.Q = 4 * S;
-  L.R = q.tail_rows;
+  L.J = srv_job_capacity(S);
   L.k_max = q.k_max;
-  L.P = max_patterns(q.k_max > q.tail_rows ? q.k_max - q.tail_rows : 0);
-  L.basis_off = a256(sizeof(SrvSlotHdr));
-  L.cum_off = L.basis_off + a256(size_t(q.k_max) * 3 * sizeof(V6));
-  L.info_off = L.cum_off + a256(size_t(L.P) * sizeof(uint64_t));
-  L.slot_bytes = L.info_off + a256(size_t(L.P) * sizeof(uint32_t));
+  L.rows_off = a256(sizeof(SrvSlotHdr));
+  L.slot_bytes = L.rows_off + a256(size_t(q.k_max) * kIsVecPerRow * sizeof(V6));
   L.table_cap = q.table_capacity > 0 ? static_cast<unsigned long long>(q.table_capacity) : 0ull;
   size_t off = 0;
   L.d_hdr = off;   off = a256(off + sizeof(SrvDevHeader));
   L.d_slots = off; off = a256(off + size_t(S) * L.slot_bytes);
-  L.d_ring = off;  off = a256(off + size_t(L.Q) * 8);
+  L.d_jobs = off;  off = a256(off + size_t(L.J) * 8);
   L.d_keys = off;  off = a256(off + L.table_cap * 8);
   L.d_vals = off;  off = a256(off + L.table_cap * 8);
   L.d_total = off;
@@ -108,7 +110,8 @@ static int srv_slots(const tg_server_params& q, int* S) {
   const SrvLayout one = srv_layout(q, 1);
   const double budget = double(free_b) * q.memory_fraction -
                         double(one.table_cap) * 16.0 - 4096.0;
-  long long s = budget > 0 ? static_cast<long long>(budget / double(one.slot_bytes)) : 0;
+  // a slot and its share of the job ring
+  long long s = budget > 0 ? static_cast<long long>(budget / double(one.slot_bytes + 512)) : 0;
   s = std::min<long long>(s, 1 << 16);
   if (s < 1) {
     set_last_error("not enough free device memory for one request slot");
@@ -246,17 +249,16 @@ int tg_server_create(tg_context* ctx, const tg_server_params* p, void* d_arena,
   a.dh = reinterpret_cast<SrvDevHeader*>(srv->d_arena + L.d_hdr);
   a.slots = srv->d_arena + L.d_slots;
   a.slot_bytes = L.slot_bytes;
-  a.basis_off = L.basis_off;
-  a.cum_off = L.cum_off;
-  a.info_off = L.info_off;
-  a.ring = reinterpret_cast<unsigned long long*>(srv->d_arena + L.d_ring);
+  a.rows_off = L.rows_off;
+  a.jobs = reinterpret_cast<unsigned long long*>(srv->d_arena + L.d_jobs);
+  a.J = L.J;
   a.keys = reinterpret_cast<unsigned long long*>(srv->d_arena + L.d_keys);
   a.vals = reinterpret_cast<unsigned long long*>(srv->d_arena + L.d_vals);
   a.table_cap = L.table_cap;
   a.S = S;
   a.Q = L.Q;
   a.k_max = q.k_max;
-  a.R = q.tail_rows;
+  a.lanes = ctx->sm_count * q.blocks_per_sm * kSrvTPB;
   a.idle_ns = static_cast<unsigned long long>(q.idle_us) * 1000ull;
   a.life_ns = static_cast<unsigned long long>(q.life_ms) * 1000000ull;
   a.tab.M = ctx->d_M;
@@ -264,7 +266,6 @@ int tg_server_create(tg_context* ctx, const tg_server_params* p, void* d_arena,
   e = cudaStreamCreateWithFlags(&srv->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&srv->aux, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaMemsetAsync(srv->d_arena, 0, L.d_total, srv->aux);
-  if (e == cudaSuccess) e = cudaMemsetAsync(a.ring, 0xFF, size_t(L.Q) * 8, srv->aux);
   if (e == cudaSuccess && L.table_cap)
     e = cudaMemsetAsync(a.keys, 0xFF, L.table_cap * 8, srv->aux);
   if (e == cudaSuccess) e = cudaStreamSynchronize(srv->aux);
@@ -324,6 +325,19 @@ int tg_server_submit(tg_server* srv, const int32_t* h_indices, int32_t k, int32_
   srv->busy_ids.push_back(id);
   srv->next_id = id + 1u;
   if (h_id) *h_id = id;
+  return TG_OK;
+}
+
+int tg_server_debug_skip_publication(tg_server* srv) {
+  if (!srv) {
+    set_last_error("tg_server_debug_skip_publication: NULL server");
+    return TG_ERR_INVALID_ARGUMENT;
+  }
+  std::lock_guard<std::mutex> lock(srv->mu);
+  const uint32_t id = srv->next_id;
+  std::atomic_thread_fence(std::memory_order_release);
+  __atomic_store_n(&srv->h_ctl->published, id + 1u, __ATOMIC_RELEASE);
+  srv->next_id = id + 1u;
   return TG_OK;
 }
 

@@ -9,16 +9,17 @@ future per request.
 
 What the loop does per request, on the GPU:
   * admission: requests take one of a fixed pool of device slots, sized from
-    free device memory; when all are busy they wait here, on the host, and
-    enter as answers free slots;
+    free device memory; when all are busy they wait here, on the host
+    (bounded by max_pending, cancellable), and enter as answers free slots;
   * canonical dedup: the AGL2(F7) canonical mask keys a device hash table; a
     request whose equivalent was already answered is answered from it when
     that answer decides this request's threshold (an exact earlier value, or
     an earlier failure whose witness exceeds this threshold); a request whose
     equivalent is still running waits for it;
-  * evaluation: the tasks of every admitted request share one persistent
-    grid, oldest request first, so requests that arrive while others run
-    overlap with them on the device (continuous batching).
+  * evaluation: by information sets, level by level; the open levels of
+    every admitted request are jobs of one device ring whose tasks the
+    warps of one persistent grid claim oldest first, so requests that arrive
+    while others run overlap with them on the device (continuous batching).
 Answers follow the batch oracle's contract: `passed` (max_zeros <= 49 - td,
 value exact) or a failure witness above 49 - td.
 """
@@ -62,7 +63,7 @@ class ToricServer:
     def __init__(self, device_id: int = 0, M: np.ndarray | None = None, *, k_max: int = 15,
                  max_slots: int = 0, memory_fraction: float = 0.25, tail_rows: int = 0,
                  table_capacity: int = 0, idle_us: int = 0, life_ms: int = 0,
-                 blocks_per_sm: int = 0):
+                 blocks_per_sm: int = 0, max_pending: int = 0):
         self.ctx = ToricContext(device_id, build_eval_matrix() if M is None else M)
         self.device = torch.device("cuda", device_id)
         lib = _lib.load()
@@ -86,6 +87,7 @@ class ToricServer:
                                         ctypes.byref(handle)), "tg_server_create")
         self.handle = handle
         self.k_max = k_max
+        self.max_pending = max_pending  # host queue bound; 0 = unbounded
         self._pending: deque = deque()
         self._inflight: dict[int, tuple[Future, float]] = {}
         self._cv = threading.Condition()
@@ -110,6 +112,9 @@ class ToricServer:
                 raise RuntimeError("server is closed")
             if self._error is not None:
                 raise RuntimeError("server failed") from self._error
+            if self.max_pending and len(self._pending) >= self.max_pending:
+                raise _lib.ToricLibError(_lib.TG_ERR_CAPACITY,
+                                         f"{len(self._pending)} requests already wait for a slot")
             self._pending.append((idx, int(target_distance), fut, time.perf_counter()))
             self._cv.notify()
         return fut
@@ -118,6 +123,17 @@ class ToricServer:
         """Submits (indices, target_distance) pairs and waits for all answers."""
         futs = [self.submit(s, td) for s, td in requests]
         return [f.result(timeout=timeout) for f in futs]
+
+    def cancel(self, fut: Future) -> bool:
+        """Cancels a request still waiting on the host for a free slot; a
+        request already admitted to the device runs to its answer.  Returns
+        True when the request was cancelled."""
+        with self._cv:
+            for i, item in enumerate(self._pending):
+                if item[2] is fut:
+                    del self._pending[i]
+                    return fut.cancel()
+        return False
 
     def stats(self) -> dict:
         c = (ctypes.c_uint64 * 8)()

@@ -300,8 +300,11 @@ int tg_hashset_insert(void* d_table, int64_t capacity, const uint64_t* d_keys,
 /* A server evaluates max_zeros requests as they arrive: requests are admitted
  * into a fixed pool of device slots (sized from free device memory), each is
  * deduplicated by its AGL2(F7) canonical form in a device hash table, carries
- * its own early-exit threshold, and has its tasks interleaved with those of
- * the requests already on the GPU by one persistent loop kernel.  This is the
+ * its own early-exit threshold, and is evaluated by information sets level
+ * by level; every open level of every request is a job of one device ring,
+ * whose tasks the warps of one persistent loop kernel claim in arrival order,
+ * so the work of requests admitted at different times overlaps on the GPU.
+ * This is the
  * B200 form of the reference's host pipeline _pipelined_eval + _dispatch
  * (champion_search_canonical.py:281-378, 237-271) and evolve_search's
  * evaluate_sets (evolve_search.py:266-282), request by request. */
@@ -311,8 +314,8 @@ typedef struct tg_server tg_server;
 typedef struct tg_server_params {
   int32_t max_slots;       /* request slots; 0 = from free device memory     */
   int32_t k_max;           /* largest request size, <= 21                    */
-  int32_t tail_rows;       /* R of the task walk; 0 = 4                      */
-  int32_t blocks_per_sm;   /* loop CTAs (128 threads) per SM; 0 = 8          */
+  int32_t tail_rows;       /* unused by the information-set loop; 0 or 2..7  */
+  int32_t blocks_per_sm;   /* loop CTAs (128 threads) per SM, 1..5; 0 = 5    */
   int32_t idle_us;         /* the loop exits after this long without work; 0 = 2000 */
   int32_t life_ms;         /* one loop launch ends after this long; 0 = 250  */
   int64_t table_capacity;  /* dedup table slots, power of two; 0 = 2^20; -1 = no dedup */
@@ -350,8 +353,15 @@ int tg_server_pump(tg_server* srv, int32_t* h_running);
 /* Collects up to max finished results (in completion order) and frees slots. */
 int tg_server_poll(tg_server* srv, tg_server_result* h_out, int32_t max, int32_t* h_n);
 /* Counters: [0] published, [1] finished, [2] outstanding, [3] loop launches,
- * [4] tasks run, [5] codewords planned, [6] dedup answers, [7] device status. */
+ * [4] level tasks run, [5] codewords evaluated, [6] dedup answers, [7] device
+ * status. */
 int tg_server_stats(tg_server* srv, uint64_t* h_counters8);
+/* Fault injection for failure tests: moves the publication counter past one
+ * request id without publishing that request.  The loop's bounded wait for
+ * the missing publication entry runs out (a few milliseconds) and sets
+ * TG_ERR_STATE in the device status (tg_server_stats counter 7); the loop and
+ * the requests published after it go on.  No counterpart in the reference. */
+int tg_server_debug_skip_publication(tg_server* srv);
 /* Stops the loop (bounded wait) and frees the server object. */
 int tg_server_destroy(tg_server* srv);
 

@@ -34,15 +34,18 @@ def same_answer(a, b_mz, td):
 
 
 def test_alone_equals_mix_equals_batch(server, gpu_oracle):
+    """Requests of the served stream's sizes (k = 10..15, thresholds around
+    the best-known distances) give the batch oracle's answer alone and when
+    interleaved with 200 others in flight together."""
     rng = random.Random(1234)
     reqs = []
     for _ in range(60):
-        k = rng.randint(3, 10)
-        reqs.append((sorted(rng.sample(range(N), k)), rng.choice([1, 20, 28, 34, 40])))
+        k = rng.randint(10, 15)
+        reqs.append((sorted(rng.sample(range(N), k)), rng.choice([1, 18, 21, 24, 26, 28])))
     exact = gpu_oracle.max_zeros_batch([s for s, _ in reqs], 1)
     alone = [server.submit(s, td).result(timeout=120) for s, td in reqs]
     # the same requests interleaved with 200 unrelated ones, all in flight together
-    noise = [(sorted(rng.sample(range(N), rng.randint(6, 12))), rng.randint(1, 40))
+    noise = [(sorted(rng.sample(range(N), rng.randint(3, 15))), rng.randint(1, 30))
              for _ in range(200)]
     mixed_reqs, mine_at = [], []
     for i, r in enumerate(reqs):
