@@ -366,7 +366,7 @@ def random_masks(n: int, k_lo: int, k_hi: int, seed: int) -> np.ndarray:
     return (bits.astype(np.uint64) << np.arange(49, dtype=np.uint64)).sum(axis=1, dtype=np.uint64)
 
 
-def bench_canonical(dev: int, n: int = 1_000_000) -> dict:
+def bench_canonical(dev: int, n: int = 1_000_000, with_cpu: bool = True) -> dict:
     """Canonical forms of n seeded 49-bit sets (popcount U{5..30}) and device
     dedup of the canonical masks."""
     import torch
@@ -398,9 +398,212 @@ def bench_canonical(dev: int, n: int = 1_000_000) -> dict:
     torch.cuda.synchronize()
     t_canon = e[0].elapsed_time(e[1]) / 1e3
     t_dedup = e[2].elapsed_time(e[3]) / 1e3
-    return {"workload": f"{n:,} seeded 49-bit sets, popcount U{{5..30}}",
-            "canonical_sets_per_s": n / t_canon, "canonical_ms": 1e3 * t_canon,
-            "dedup_ms": 1e3 * t_dedup, "unique": int(n_new.item())}
+    out = {"workload": f"{n:,} seeded 49-bit sets, popcount U{{5..30}}",
+           "canonical_sets_per_s": n / t_canon, "canonical_ms": 1e3 * t_canon,
+           "dedup_ms": 1e3 * t_dedup, "unique": int(n_new.item())}
+    out["reference_gpu"] = canonical_reference_kernel(dev, masks, co, lib)
+    if with_cpu:
+        out["cpu_baseline"] = canonical_cpu_baseline(masks)
+    return out
+
+
+def _rows_of(masks: np.ndarray) -> list[list[int]]:
+    return [[i for i in range(49) if (int(m) >> i) & 1] for m in masks.tolist()]
+
+
+def canonical_reference_kernel(dev: int, masks: np.ndarray, co, lib, n: int = 200_000) -> dict:
+    """The reference canonical kernel (kernel_canon.py:44-129, one warp per
+    set, one launch per set size as CanonicalOracle.compute takes (n, k)
+    arrays) against this repository's on the same sets: the first n masks of
+    popcount <= 16 (the reference key's limit), grouped by popcount."""
+    import torch
+
+    from generalized_toric_gpu_search_b200 import _lib
+    from generalized_toric_gpu_search_b200.tables import precompute_gl2_perms, rel_table
+
+    ref = _ref_kernels()
+    if ref is None:
+        return {"unavailable": "oracle/_ref/libref_kernels.so not built"}
+    device = torch.device("cuda", dev)
+    pc = np.array([bin(int(m)).count("1") for m in masks[: 4 * n].tolist()])
+    sel = masks[: 4 * n][pc <= 16][:n]
+    rows = _rows_of(sel)
+    by_k: dict[int, list] = {}
+    for r in rows:
+        by_k.setdefault(len(r), []).append(r)
+    perms = torch.from_numpy(precompute_gl2_perms()).to(device)
+    rel = torch.from_numpy(rel_table()).to(device)
+    st = torch.cuda.current_stream(device)
+    t_ref = t_ours = 0.0
+    for k, group in sorted(by_k.items()):
+        d_sets = torch.tensor(group, dtype=torch.int32, device=device)
+        m = len(group)
+        lo = torch.full((m,), -1, dtype=torch.int64, device=device)
+        hi = torch.zeros(m, dtype=torch.int64, device=device)
+        om = torch.empty(m, dtype=torch.int64, device=device)
+        ol, oh = torch.empty_like(om), torch.empty_like(om)
+        for rep_ in range(2):  # the first pass warms both modules
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            e[0].record(st)
+            ref.ref_canon(d_sets.data_ptr(), perms.data_ptr(), rel.data_ptr(), lo.data_ptr(),
+                          hi.data_ptr(), m, k, st.cuda_stream)
+            e[1].record(st)
+            _lib.check(lib.tg_canonical_sets(co.ctx.handle, d_sets.data_ptr(), m, k,
+                                             om.data_ptr(), ol.data_ptr(), oh.data_ptr(), None,
+                                             st.cuda_stream), "tg_canonical_sets")
+            e[2].record(st)
+            e[2].synchronize()
+        t_ref += e[0].elapsed_time(e[1]) / 1e3
+        t_ours += e[1].elapsed_time(e[2]) / 1e3
+        if not (torch.equal(lo, ol) and torch.equal(hi, oh)):
+            raise SystemExit(f"canonical keys differ from the reference kernel at k = {k}")
+    return {"sets": len(rows), "sample": f"first {len(rows):,} masks with popcount <= 16, one "
+                                         "launch per popcount",
+            "reference_sets_per_s": len(rows) / t_ref, "ours_sets_per_s": len(rows) / t_ours,
+            "speedup": t_ref / t_ours, "keys_equal": True}
+
+
+def _numpy_canonical_chunk(args):
+    from oracle import oracle as orc
+
+    k, rows = args
+    return len(orc.canonical_forms_numpy(np.array(rows, dtype=np.int32)))
+
+
+def canonical_cpu_baseline(masks: np.ndarray, n_c: int = 200_000, n_np: int = 8_000) -> dict:
+    """CPU baselines of the canonical form on the host's cores: the C
+    restatement of kernel_canon.py (OpenMP, every popcount) on the first n_c
+    masks, and the numpy restatement of the reference's canonical_forms_batch
+    (champion_search_canonical.py:115-140, k <= 10) in a process pool of one
+    worker per core on the first n_np masks of popcount <= 10."""
+    import multiprocessing as mp
+
+    from oracle import oracle as orc
+
+    cores = os.cpu_count() or 1
+    sub = masks[:n_c]
+    t0 = time.perf_counter()
+    orc.canonical_masks(sub, threads=cores)
+    t_c = time.perf_counter() - t0
+    pc = np.array([bin(int(m)).count("1") for m in masks[: 4 * n_np].tolist()])
+    rows = _rows_of(masks[: 4 * n_np][pc <= 10][:n_np])
+    chunks = []
+    by_k: dict[int, list] = {}
+    for r in rows:
+        by_k.setdefault(len(r), []).append(r)
+    for k, group in by_k.items():
+        step = max(1, len(group) // cores + 1)
+        chunks += [(k, group[i:i + step]) for i in range(0, len(group), step)]
+    with mp.get_context("spawn").Pool(cores) as pool:
+        pool.map(_numpy_canonical_chunk, [(5, [[0, 1, 2, 3, 4]])] * cores)  # start the workers
+        t0 = time.perf_counter()
+        done = sum(pool.map(_numpy_canonical_chunk, chunks))
+        t_np = time.perf_counter() - t0
+    return {"value": len(sub) / t_c, "unit": "sets/s", "cores": cores, "kind": "port",
+            "sample": f"first {len(sub):,} masks (popcount 5..30), C restatement, OpenMP",
+            "numpy_reference_restated": {"value": done / t_np, "unit": "sets/s",
+                                         "cores": cores,
+                                         "sample": f"first {done:,} masks of popcount <= 10, "
+                                                   "canonical_forms_batch restated in numpy, "
+                                                   "spawn pool of one process per core"}}
+
+
+REF_LIB = ROOT / "oracle" / "_ref" / "libref_kernels.so"
+
+
+def _ref_kernels():
+    """The reference's own CUDA kernels, built from its kernel source by
+    oracle/build_ref.py and launched with its wrappers' geometry by
+    oracle/ref_harness.cu (a baseline here, never the measured product), or
+    None when the library was not built."""
+    import ctypes
+
+    if not REF_LIB.exists():
+        return None
+    lib = ctypes.CDLL(str(REF_LIB))
+    vp = ctypes.c_void_p
+    lib.ref_bp_batch.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                 ctypes.c_longlong, ctypes.c_ulonglong, vp, vp]
+    lib.ref_bp_single.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, vp, vp]
+    lib.ref_canon.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int, ctypes.c_int, vp]
+    return lib
+
+
+def bench_reference_gpu(dev: int, sets, full: int = 1184, ks=(6, 7, 8, 9)) -> dict:
+    """The plain GPU form of the reference on this B200:
+    eval_min_distance_batch_bp (kernel_cuda_bp.py:146-238), one launch per
+    uniform-k group (the only batching its max_zeros_batch offers), and
+    eval_min_distance_single_bp (:266-288), one launch per code.  Each is
+    timed with CUDA events at k = 6..9 -- the batch kernel on `full` sets per
+    launch (8 blocks of 256 threads per SM, full occupancy), the single-set
+    kernel on 4 codes per k.  A full launch above k = 9 takes from ~10 s to
+    hours, so the time per message at k = 10..14 comes from the least-squares
+    line t(k) = a + b k through the measured k (the inner loop is k
+    shared-memory lookups per message), applied to the workload's k mix."""
+    import torch
+
+    from generalized_toric_gpu_search_b200.tables import build_eval_matrix
+
+    lib = _ref_kernels()
+    if lib is None:
+        return {"unavailable": "oracle/_ref/libref_kernels.so not built"}
+    device = torch.device("cuda", dev)
+    d_M = torch.from_numpy(np.ascontiguousarray(build_eval_matrix().astype(np.int32))).to(device)
+    st = torch.cuda.current_stream(device)
+    by_k: dict[int, list] = {}
+    for s_ in sets:
+        by_k.setdefault(len(s_), []).append(s_)
+
+    def timed(fn) -> float:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        fn()
+        e1.record(st)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / 1e3
+
+    batch_t, single_t = {}, {}
+    for k in ks:
+        group = by_k[k]
+        rows = [group[i % len(group)] for i in range(full)]
+        flat = torch.tensor([i for r in rows for i in r], dtype=torch.int32, device=device)
+        out = torch.zeros(full, dtype=torch.int32, device=device)
+        lib.ref_bp_batch(d_M.data_ptr(), flat.data_ptr(), k, 48, 8, 0, 0, out.data_ptr(),
+                         st.cuda_stream)  # warm-up launch
+        secs = timed(lambda: lib.ref_bp_batch(d_M.data_ptr(), flat.data_ptr(), k, 48, full, 0, 0,
+                                              out.data_ptr(), st.cuda_stream))
+        batch_t[k] = secs / (full * float(8 ** k - 1))
+        one = torch.zeros(1, dtype=torch.int32, device=device)
+        tot = 0.0
+        for r in group[:4]:
+            d_s = torch.tensor(r, dtype=torch.int32, device=device)
+            one.zero_()
+            tot += timed(lambda: lib.ref_bp_single(d_M.data_ptr(), d_s.data_ptr(), k, 48,
+                                                   one.data_ptr(), st.cuda_stream))
+        single_t[k] = tot / (4 * float(8 ** k - 1))
+    hist = k_histogram(sets)
+    msgs = sum(hist[k] * float(8 ** k - 1) for k in hist)
+
+    def total_seconds(t_by_k):
+        kk = np.array(sorted(t_by_k), dtype=np.float64)
+        b, a = np.polyfit(kk, np.array([t_by_k[int(k)] for k in kk]), 1)
+        per = {k: (t_by_k[k] if k in t_by_k else a + b * k) for k in hist}
+        return sum(hist[k] * float(8 ** k - 1) * per[k] for k in hist), per
+
+    batch_s, batch_per = total_seconds(batch_t)
+    single_s, single_per = total_seconds(single_t)
+    return {"kernel": "reference eval_min_distance_batch_bp / eval_min_distance_single_bp "
+                      "(built from kernel_cuda_bp.py's source for sm_100a)",
+            "batched_per_k_launch": {"value": msgs / batch_s, "unit": UNIT,
+                                     "messages_per_s_measured": {k: 1.0 / t for k, t in
+                                                                 batch_t.items()}},
+            "one_code_per_launch": {"value": msgs / single_s, "unit": UNIT,
+                                    "messages_per_s_measured": {k: 1.0 / t for k, t in
+                                                                single_t.items()}},
+            "step_seconds_batched": batch_s, "step_seconds_one_per_launch": single_s,
+            "sample": f"measured at k = {list(ks)} ({full} sets per batch launch, 4 single-set "
+                      f"launches per k); k = {sorted(set(hist) - set(ks))} extrapolated by "
+                      "t(k) = a + b k per message"}
 
 
 def bench_early_exit(dev: int, n: int = 2000) -> dict:
@@ -495,6 +698,18 @@ def bench_served(dev: int, n: int = 3000, rate: float = 300.0, engine: str = "ba
         tb = time.perf_counter()
         srv.evaluate([(s, best[len(s)]) for s in burst], timeout=600)
         burst_s = time.perf_counter() - tb
+    # The plain form on the same burst: one max_zeros call (one batch of one
+    # code) per request, in arrival order, on a prefix of the stream.
+    from generalized_toric_gpu_search_b200.distance import DistanceOracleCUDABP
+    from generalized_toric_gpu_search_b200.tables import build_eval_matrix
+
+    plain_o = DistanceOracleCUDABP(dev, build_eval_matrix())
+    n_plain = min(n, 500)
+    plain_o.max_zeros(burst[0], best[len(burst[0])])
+    tp = time.perf_counter()
+    for s in burst[:n_plain]:
+        plain_o.max_zeros(s, best[len(s)])
+    plain_s = time.perf_counter() - tp
     lat = np.array([a.latency_s for a in answers])
     dev_t = np.array([a.device_s for a in answers])
     return {"workload": (f"{n:,} Poisson arrivals at {rate:.0f}/s, single mutations of 256 seeded "
@@ -509,6 +724,9 @@ def bench_served(dev: int, n: int = 3000, rate: float = 300.0, engine: str = "ba
             "slots": slots, "loop_launches": st.get("loop_launches"),
             "batches": st.get("batches"),
             "burst_codes_per_s": n / burst_s,
+            "plain_one_code_per_call_codes_per_s": n_plain / plain_s,
+            "burst_vs_plain": (n / burst_s) / (n_plain / plain_s),
+            "plain_sample": f"first {n_plain} requests of the burst, one max_zeros call each",
             "best_known_d_end": best}
 
 
@@ -695,11 +913,14 @@ def run_b200_arm(args, d: Dist) -> None:
     achieved = dominant["popc_per_codeword"] * dominant["codewords"] / dominant["seconds"]
 
     extra = {}
+    ref_gpu = None
+    if d.rank == 0 and not args.skip_plain:
+        ref_gpu = bench_reference_gpu(dev, sets)
     if d.rank == 0 and not args.skip_extra:
         extra["canonical_forms"] = bench_canonical(dev)
         extra["early_exit_k15"] = bench_early_exit(dev)
-        extra["served_stream"] = bench_served(dev, engine="batch")
-        extra["served_stream_persistent"] = bench_served(dev, engine="persistent")
+        extra["served_stream"] = bench_served(dev, engine="persistent")
+        extra["served_stream_batch"] = bench_served(dev, engine="batch")
 
     cpu = None
     if d.rank == 0 and d.world == 1 and not args.skip_cpu:
@@ -738,6 +959,16 @@ def run_b200_arm(args, d: Dist) -> None:
             "clocks": clk,
             "plain_form": plain,
             "batched_vs_plain": (value / plain["value"]) if plain else None,
+            "reference_gpu": ref_gpu,
+            "batched_vs_reference_gpu": (value / ref_gpu["batched_per_k_launch"]["value"])
+            if ref_gpu and "batched_per_k_launch" in ref_gpu else None,
+            "batched_vs_reference_gpu_one_per_launch":
+                (value / ref_gpu["one_code_per_launch"]["value"])
+                if ref_gpu and "one_code_per_launch" in ref_gpu else None,
+            # the reference's enumeration (all 8^k - 1 messages) on the B200 and on
+            # the host cores: a hardware-only ratio of the same algorithm
+            "same_algorithm_gpu_vs_cpu": (ref_gpu["batched_per_k_launch"]["value"] / cpu["value"])
+            if ref_gpu and "batched_per_k_launch" in ref_gpu and cpu else None,
             "cpu_baseline": cpu,
             **extra,
         }
@@ -763,7 +994,8 @@ def main(argv=None) -> None:
     ap.add_argument("--n-sets", type=int, default=N_SETS, help="sets per GPU (small cases)")
     ap.add_argument("--kmin", type=int, default=K_LO)
     ap.add_argument("--kmax", type=int, default=K_HI)
-    ap.add_argument("--section", choices=["canonical", "early-exit", "served", "served-persistent"],
+    ap.add_argument("--section", choices=["canonical", "early-exit", "served", "served-persistent",
+                                          "reference-gpu"],
                     help="run one secondary configuration alone and print its JSON")
     ap.add_argument("--canon-n", type=int, default=1_000_000)
     args = ap.parse_args(argv)
@@ -775,7 +1007,8 @@ def main(argv=None) -> None:
         fn = {"canonical": lambda: bench_canonical(0, args.canon_n),
               "early-exit": lambda: bench_early_exit(0),
               "served": lambda: bench_served(0, engine="batch"),
-              "served-persistent": lambda: bench_served(0, engine="persistent")}[args.section]
+              "served-persistent": lambda: bench_served(0, engine="persistent"),
+              "reference-gpu": lambda: bench_reference_gpu(0, make_workload(0))}[args.section]
         print(json.dumps({"section": args.section, **fn()}), flush=True)
         return
     if args.impl == "reference":
