@@ -774,10 +774,21 @@ def run_b200_arm(args, d: Dist) -> None:
     sets = make_workload(d.rank, args.n_sets, args.kmin, args.kmax)
     M = build_eval_matrix()
     ctx = ToricContext(dev, M)
-    cfg = LaunchConfig(tail_rows=args.tail_rows, blocks_per_sm=args.blocks_per_sm,
-                       enumeration=ENUMERATIONS[args.enumeration][0])
-    runner = DistanceRunner(ctx, cfg)
     flat, offsets, kmax = pack_sets(sets)
+    # The launch shape the autotuner picked for this batch's largest k (tuned
+    # here first when the device has no table), with the command line's
+    # orbit-walk overrides.
+    from dataclasses import asdict, replace
+
+    from generalized_toric_gpu_search_b200 import autotune
+
+    tuned = autotune.choose(autotune.ensure_table(dev), kmax) if not args.no_autotune else None
+    cfg = replace(tuned or LaunchConfig(), enumeration=ENUMERATIONS[args.enumeration][0])
+    if args.tail_rows:
+        cfg = replace(cfg, tail_rows=args.tail_rows)
+    if args.blocks_per_sm:
+        cfg = replace(cfg, blocks_per_sm=args.blocks_per_sm)
+    runner = DistanceRunner(ctx, cfg)
     d_idx = torch.from_numpy(flat).to(device)
     d_off = torch.from_numpy(offsets).to(device)
     d_out = torch.empty(len(sets), dtype=torch.int32, device=device)
@@ -938,6 +949,10 @@ def run_b200_arm(args, d: Dist) -> None:
                        "enumeration": ENUMERATIONS[args.enumeration][1],
                        "variant": "histogram", "tail_rows": args.tail_rows or 4,
                        "launch": "CUDA graphs: prepare, enumeration walk, information-set walk",
+                       "launch_shape": {k_: v for k_, v in asdict(cfg).items()
+                                        if k_ not in ("enumeration", "variant")},
+                       "launch_shape_source": ("autotuned for k = %d (0 = library default)"
+                                               % kmax) if tuned else "library defaults",
                        "l2": "256 MiB write between timed steps",
                        "parallelism": f"weak, {d.world} rank(s), no data-path collective"},
             "codes_per_s": d.world * len(sets) / (total_ms / 1e3 / args.steps),
@@ -988,6 +1003,8 @@ def main(argv=None) -> None:
     ap.add_argument("--enumeration", choices=sorted(ENUMERATIONS), default="auto",
                     help="exact enumeration of the headline workload")
     ap.add_argument("--skip-plain", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="library default launch shapes instead of the tuned ones")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-extra", action="store_true",
                     help="skip the canonical, early-exit and served-stream sections")

@@ -162,6 +162,10 @@ class DistanceParams(ctypes.Structure):
         ("target_distance", c_int32),
         ("sample_count", c_int64),
         ("sample_seed", c_uint64),
+        ("is_blocks_per_sm", c_int32),
+        ("is_tasks_per_thread", c_int32),
+        ("is_max_task_units", c_int32),
+        ("is_pad", c_int32),
     ]
 
 

@@ -1,15 +1,23 @@
-"""Per-k launch-shape autotuner of the batched max_zeros kernel.
+"""Per-k launch-shape autotuner of the batched max_zeros kernels.
 
-The persistent walk has three shape knobs:
-  tail_rows R        -- one task covers the 8^R codewords of the last R rows,
-                        so R sets the equal-cost slice size (512 .. 32768);
+The information-set walk (the default enumeration for k >= 2) has three
+knobs, tuned per k:
+  is_blocks_per_sm     -- resident CTAs of 128 threads per SM (1..5);
+  is_tasks_per_thread  -- a level is cut into about this many tasks per
+                          resident thread (the equal-cost slice count);
+  is_max_task_units    -- the largest task, in 49-codeword blocks (the slice
+                          size cap; tasks align with supports).
+The orbit walk (k = 1 by default, every k under TG_ENUM_ORBIT) has three:
+  tail_rows R        -- one task covers the 8^R codewords of the last R rows;
   blocks_per_sm      -- resident CTAs per SM (register budget 128 or 64);
   threads_per_block  -- 64 / 128 / 256 threads per CTA.
 Codes are not pinned to CTAs: every warp claims 32 tasks at a time from one
 queue, so codes per CTA follow from the task size.  `tune` times every
-candidate shape on a seeded calibration batch per k and records the fastest
-in a JSON cache keyed by the GPU name; `config_for` returns the cached shape
-for a batch (by its largest k) and the oracles pick it up automatically.
+candidate on a seeded calibration batch per k and records the fastest in a
+JSON cache keyed by the GPU name; `ensure_table` tunes the information-set
+knobs of the k it lacks (a few seconds), which DistanceOracleCUDABP does at
+first use on a device without a table; `choose` returns the shape for a
+batch by its largest k.
 """
 
 from __future__ import annotations
@@ -28,6 +36,17 @@ CANDIDATES = [
     for r in (3, 4, 5)
     for (b, t) in ((8, 128), (4, 128), (4, 256), (16, 64))
 ]
+
+INFOSET_CANDIDATES = [
+    dict(is_blocks_per_sm=b, is_tasks_per_thread=f, is_max_task_units=u)
+    for b in (4, 5)
+    for f in (4, 8, 16)
+    for u in (49, 343, 2401)
+]
+
+INFOSET_KS = range(6, 16)
+_SHAPE_KEYS = ("tail_rows", "blocks_per_sm", "threads_per_block", "is_blocks_per_sm",
+               "is_tasks_per_thread", "is_max_task_units")
 
 
 def cache_path() -> Path:
@@ -65,15 +84,15 @@ def save_table(device_name: str, table: dict[int, dict], path: Path | None = Non
 
 def choose(table: dict[int, dict], k_max: int) -> LaunchConfig | None:
     """Shape for a batch whose largest set has k_max rows: the entry of the
-    nearest tuned k at or below k_max (work is dominated by the largest k)."""
+    nearest tuned k at or below k_max (work is dominated by the largest k);
+    knobs an entry does not hold keep the library defaults."""
     if not table:
         return None
     ks = sorted(table)
     below = [k for k in ks if k <= k_max]
     k = below[-1] if below else ks[0]
     e = table[k]
-    return LaunchConfig(tail_rows=int(e["tail_rows"]), blocks_per_sm=int(e["blocks_per_sm"]),
-                        threads_per_block=int(e["threads_per_block"]))
+    return LaunchConfig(**{key: int(e[key]) for key in _SHAPE_KEYS if key in e})
 
 
 def config_for(device_id: int, k_max: int, path: Path | None = None) -> LaunchConfig | None:
@@ -87,6 +106,13 @@ def calibration_sets(k: int, target_codewords: float = 2e10, seed: int = 97) -> 
     """Seeded sets of size k whose orbit enumeration is ~target_codewords."""
     per_code = max(1.0, 0.2 * 8.0 ** max(k - 2, 1))
     n = int(min(4096, max(148, target_codewords / per_code)))
+    rng = np.random.default_rng(seed + k)
+    return [sorted(rng.choice(49, k, replace=False).tolist()) for _ in range(n)]
+
+
+def infoset_calibration_sets(k: int, seed: int = 197) -> list[list[int]]:
+    """Seeded sets of size k for the information-set walk (a few ms a batch)."""
+    n = 4096 if k <= 9 else 1024
     rng = np.random.default_rng(seed + k)
     return [sorted(rng.choice(49, k, replace=False).tolist()) for _ in range(n)]
 
@@ -118,30 +144,52 @@ def measure(runner_factory, sets, config: LaunchConfig, reps: int = 2) -> float:
 
 
 def tune(device_id: int = 0, ks=range(6, 16), candidates=None, path: Path | None = None,
-         verbose: bool = False) -> dict[int, dict]:
-    """Times every candidate shape per k and stores the fastest."""
+         verbose: bool = False, walk: str = "orbit") -> dict[int, dict]:
+    """Times every candidate shape per k and stores the fastest.  walk
+    "orbit" tunes the orbit walk's knobs (enumeration TG_ENUM_ORBIT),
+    "infoset" the information-set walk's (the default enumeration); the
+    knobs of the other walk in a table entry are kept."""
     from . import _lib
     from .distance import DistanceRunner, ToricContext
     from .tables import build_eval_matrix
 
-    cands = candidates or CANDIDATES
+    infoset = walk == "infoset"
+    cands = candidates or (INFOSET_CANDIDATES if infoset else CANDIDATES)
     ctx = ToricContext(device_id, build_eval_matrix())
     name = _lib.device_info(device_id)[3]
     table = load_table(name, path)
     for k in ks:
-        sets = calibration_sets(k)
+        sets = infoset_calibration_sets(k) if infoset else calibration_sets(k)
         results = []
         for c in cands:
-            if c["tail_rows"] > k:
+            if c.get("tail_rows", 0) > k:
                 continue
-            cfg = LaunchConfig(**c)
+            cfg = LaunchConfig(**c) if infoset else \
+                LaunchConfig(enumeration=2, **c)  # TG_ENUM_ORBIT: the walk these knobs shape
             t = measure(lambda cf: DistanceRunner(ctx, cf), sets, cfg)
             results.append((t, c))
             if verbose:
                 print(f"[autotune] k={k:2d} {c} {1e3 * t:8.3f} ms")
         t_best, c_best = min(results, key=lambda x: x[0])
-        table[k] = dict(c_best, seconds=t_best, n_sets=len(sets),
-                        tuned_at=time.strftime("%Y-%m-%dT%H:%M:%S"))
+        entry = dict(table.get(k, {}))
+        entry.update(c_best)
+        entry["infoset_seconds" if infoset else "seconds"] = t_best
+        entry["n_sets" if not infoset else "infoset_n_sets"] = len(sets)
+        entry["tuned_at"] = time.strftime("%Y-%m-%dT%H:%M:%S")
+        table[k] = entry
     save_table(name, table, path)
     ctx.close()
+    return table
+
+
+def ensure_table(device_id: int = 0, ks=INFOSET_KS, path: Path | None = None) -> dict[int, dict]:
+    """The device's table, with the information-set knobs tuned for every k
+    of ks that lacks them."""
+    from . import _lib
+
+    name = _lib.device_info(device_id)[3]
+    table = load_table(name, path)
+    missing = [k for k in ks if "is_tasks_per_thread" not in table.get(k, {})]
+    if missing:
+        table = tune(device_id, ks=missing, path=path, walk="infoset")
     return table

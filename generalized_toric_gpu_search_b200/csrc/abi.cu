@@ -222,6 +222,12 @@ static int check_distance_params(const tg_distance_params* p) {
   if (p->threads_per_block != 0 && p->threads_per_block != 64 && p->threads_per_block != 128 &&
       p->threads_per_block != 256)
     return invalid("threads_per_block must be 0, 64, 128 or 256");
+  if (p->is_blocks_per_sm < 0 || p->is_blocks_per_sm > 5)
+    return invalid("is_blocks_per_sm must be 0..5");
+  if (p->is_tasks_per_thread < 0 || p->is_tasks_per_thread > 64)
+    return invalid("is_tasks_per_thread must be 0..64");
+  if (p->is_max_task_units < 0 || p->is_max_task_units > 2401)
+    return invalid("is_max_task_units must be 0..2401");
   return TG_OK;
 }
 
@@ -300,6 +306,9 @@ static int bind_distance(tg_context* ctx, const tg_distance_params* p, const int
   a.tab.M = ctx->d_M;
   a.tab.gl2 = ctx->d_gl2;
   a.is_toric = ctx->is_toric;
+  a.is_blocks_per_sm = p->is_blocks_per_sm > 0 ? p->is_blocks_per_sm : 5;
+  a.is_tasks_per_thread = p->is_tasks_per_thread > 0 ? p->is_tasks_per_thread : 8;
+  a.is_max_task_units = p->is_max_task_units > 0 ? p->is_max_task_units : 343;
   bind_workspace(a, L, d_workspace);
   return TG_OK;
 }

@@ -895,9 +895,10 @@ int run_walk(const DistArgs& args, int sm_count, int blocks_per_sm, int tpb, cud
     // threads per SM (96 registers, no spills, 28 KB of shared memory each;
     // 6 CTAs at 80 registers spill and ran 1 % slower).  Levels no code needs
     // return before any setup.
-    constexpr int kPerSm = 5;
+    constexpr int kPerSm = 5;  // register budget of the walk (96 per thread)
     DistArgs la = args;
-    la.is_lanes = sm_count * kPerSm * kIsWalkThreads;
+    const int per_sm = args.is_blocks_per_sm > 0 ? min(args.is_blocks_per_sm, kPerSm) : kPerSm;
+    la.is_lanes = sm_count * per_sm * kIsWalkThreads;
     const int plan_grid = (args.n + 255) / 256;
     levels123_kernel<<<(args.n + 3) / 4, 128, 0, s>>>(la);
     for (int w = 4; w <= args.k_max; ++w) {
@@ -905,10 +906,10 @@ int run_walk(const DistArgs& args, int sm_count, int blocks_per_sm, int tpb, cud
       scan_level_kernel<<<1, kScanThreads, 0, s>>>(la, w);
       if (la.witness)
         walk_level_kernel<kIsWalkThreads, kPerSm, true>
-            <<<sm_count * kPerSm, kIsWalkThreads, 0, s>>>(la, w);
+            <<<sm_count * per_sm, kIsWalkThreads, 0, s>>>(la, w);
       else
         walk_level_kernel<kIsWalkThreads, kPerSm, false>
-            <<<sm_count * kPerSm, kIsWalkThreads, 0, s>>>(la, w);
+            <<<sm_count * per_sm, kIsWalkThreads, 0, s>>>(la, w);
     }
     finalize_infoset_kernel<<<plan_grid, 256, 0, s>>>(la);
     e = cudaGetLastError();

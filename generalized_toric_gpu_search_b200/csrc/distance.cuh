@@ -96,6 +96,9 @@ struct DistArgs {
   int is_toric;                  // M is the toric matrix (torus translations are automorphisms)
   int is_stride;                 // V6 per code in is_rows
   int is_lanes;                  // resident threads of the walk (task sizing)
+  int is_blocks_per_sm;          // walk CTAs per SM
+  int is_tasks_per_thread;       // tasks per resident thread a level is cut into
+  int is_max_task_units;         // largest task, in blocks
   IsHeader* is_hdr;              // task queue of the information-set walk
   V6* is_rows;                   // per code and set: k rows x (g, 6 deltas)
   uint64_t* is_units;            // units of the current level per code

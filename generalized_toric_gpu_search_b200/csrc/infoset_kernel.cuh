@@ -385,9 +385,12 @@ __global__ void __launch_bounds__(kScanThreads) scan_level_kernel(DistArgs a, in
       if (tot + s_part[i] < tot) s_over = 1;
       tot += s_part[i];
     }
-    const unsigned long long target = 8ull * static_cast<unsigned long long>(a.is_lanes);
+    const unsigned long long target = static_cast<unsigned long long>(a.is_tasks_per_thread) *
+                                      static_cast<unsigned long long>(a.is_lanes);
     unsigned long long nb = (tot + target - 1ull) / target;
-    nb = max(1ull, min(nb, is_max_task_units(w)));
+    // the largest task: the tunable limit from level 3 on (343 by default)
+    nb = max(1ull, min(nb, w >= 3 ? static_cast<unsigned long long>(a.is_max_task_units)
+                                  : is_max_task_units(w)));
     // Align tasks with supports (units per support is a power of 7): whole
     // supports, or the power of 7 dividing one that is nearest on a log
     // scale, so the lanes of a warp walk equal block counts.

@@ -42,6 +42,11 @@ class LaunchConfig:
     variant: int = _lib.TG_VARIANT_AUTO
     blocks_per_sm: int = 0
     threads_per_block: int = 0
+    # the information-set walk: CTAs per SM, tasks per resident thread of a
+    # level, largest task in 49-codeword blocks (0 = library defaults 5, 8, 343)
+    is_blocks_per_sm: int = 0
+    is_tasks_per_thread: int = 0
+    is_max_task_units: int = 0
 
 
 def _require_cuda(device_id: int) -> None:
@@ -213,6 +218,8 @@ class DistanceRunner:
             variant=c.variant, blocks_per_sm=c.blocks_per_sm,
             threads_per_block=c.threads_per_block, target_distance=int(target_distance),
             sample_count=int(sample_count), sample_seed=int(sample_seed) & (2**64 - 1),
+            is_blocks_per_sm=c.is_blocks_per_sm, is_tasks_per_thread=c.is_tasks_per_thread,
+            is_max_task_units=c.is_max_task_units,
         )
 
     def workspace(self, p: _lib.DistanceParams) -> torch.Tensor:
@@ -332,9 +339,16 @@ class DistanceOracleCUDABP:
         self._fixed = config
         self._table: dict = {}
         if config is None and autotune:
-            from .autotune import load_table
+            import os
 
-            self._table = load_table(_lib.device_info(device_id)[3])
+            from .autotune import ensure_table, load_table
+
+            # A device without a table is tuned at first use (a few seconds),
+            # unless TORIC_B200_AUTOTUNE=0 asks for the library defaults.
+            if os.environ.get("TORIC_B200_AUTOTUNE", "1") != "0":
+                self._table = ensure_table(device_id)
+            else:
+                self._table = load_table(_lib.device_info(device_id)[3])
         self._runners: dict[tuple, DistanceRunner] = {}
         self.runner = self._runner_for(0, False)
         self.device = self.runner.device
@@ -351,7 +365,8 @@ class DistanceOracleCUDABP:
             cfg = choose(self._table, k_max)
         cfg = cfg or LaunchConfig()
         key = (cfg.tail_rows, cfg.enumeration, cfg.variant, cfg.blocks_per_sm,
-               cfg.threads_per_block)
+               cfg.threads_per_block, cfg.is_blocks_per_sm, cfg.is_tasks_per_thread,
+               cfg.is_max_task_units)
         r = self._runners.get(key)
         if r is None:
             r = self._runners[key] = DistanceRunner(self.ctx, cfg)

@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define TG_ABI_VERSION 1
+#define TG_ABI_VERSION 2
 
 /* ---- status codes ------------------------------------------------------ */
 enum {
@@ -118,6 +118,13 @@ typedef struct tg_distance_params {
   int32_t target_distance; /* used for every set when d_target is NULL       */
   int64_t sample_count;    /* 0 = exact; > 0 = reference sampled screening   */
   uint64_t sample_seed;    /* splitmix64 seed of the sampled mode            */
+  /* Launch shape of the information-set walk (ABI version 2): */
+  int32_t is_blocks_per_sm;    /* CTAs of 128 threads per SM, 1..5; 0 = 5        */
+  int32_t is_tasks_per_thread; /* a level is cut into about this many tasks per
+                                  resident thread, 1..64; 0 = 8                  */
+  int32_t is_max_task_units;   /* largest task, in 49-codeword blocks, 1..2401;
+                                  0 = 343                                        */
+  int32_t is_pad;
 } tg_distance_params;
 
 /* Bytes of workspace tg_max_zeros needs for these parameters. */

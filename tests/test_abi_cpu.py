@@ -37,7 +37,9 @@ def test_header_matches_bindings(lib):
 def test_status_strings(lib):
     assert lib.tg_status_string(0) == b"TG_OK"
     assert lib.tg_status_string(7) == b"TG_ERR_BAD_INPUT"
-    assert lib.tg_abi_version() == 1
+    assert lib.tg_abi_version() == 2
+    # tg_distance_params grew by the information-set walk's launch knobs
+    assert ctypes.sizeof(_lib.DistanceParams) == 64
 
 
 def test_device_count_without_gpu(lib):
