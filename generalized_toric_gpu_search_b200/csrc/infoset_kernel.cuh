@@ -715,32 +715,25 @@ __device__ __forceinline__ int is_sweep_fix(uint32_t kC, const int (&z)[7], int 
   }
 // The same test on pairs of codewords: the selections of alpha^0|alpha^1,
 // alpha^2|alpha^3 and alpha^4|alpha^5 are disjoint, so each pair's count
-// bounds both of its codewords' zeros; four counts instead of seven.  The
-// count of g's zero columns where P is nonzero (which only lowers a
-// codeword's zeros) is left out, so the test is looser but needs no Pz: four
-// counts per seven codewords.  Used at high thresholds, where flags are rare:
-// bit S of fl marks the sweep, and the block's flagged sweeps are counted
-// after it, so the seven sweeps are one stretch of straight-line code.
+// bounds both of its codewords' zeros; four counts instead of seven.  Used at
+// high thresholds, where flags are rare: bit S of fl marks the sweep, and the
+// block's flagged sweeps are counted after it, so the seven sweeps are one
+// stretch of straight-line code.
 #define TG_IS_SWEEP2(S)                                                                          \
   {                                                                                              \
     const int y0_ = __popc(lop3<sel_lut(1) | sel_lut(2)>(W.x0, W.x1, W.x2));                     \
     const int y1_ = __popc(lop3<sel_lut(4) | sel_lut(3)>(W.x0, W.x1, W.x2));                     \
     const int y2_ = __popc(lop3<sel_lut(6) | sel_lut(7)>(W.x0, W.x1, W.x2));                     \
     const int y3_ = __popc(lop3<sel_lut(5)>(W.x0, W.x1, W.x2));                                  \
-    const int ym_ = __vimax3_s32(y0_, y1_, max(y2_, y3_));                                       \
+    const int pz_ = __popc(lop3<0xFE>(Pz.x0, Pz.x1, Pz.x2));                                    \
+    const int ym_ = __vimax3_s32(y0_, y1_, max(y2_, y3_)) - pz_;                                 \
     fl |= ym_ > thz ? (1u << (S)) : 0u;                                                          \
   }
-// Digit 1's move I in the W domain only (the pair test), and on g's zero
-// columns too (the single test, which tracks Pz sweep by sweep).
-#define TG_IS_MOVE_W(I)                                                      \
+#define TG_IS_MOVE(I)                                                        \
   {                                                                          \
     W.x0 ^= ez[(6 * (I) + 0) * kStride];                                     \
     W.x1 ^= ez[(6 * (I) + 1) * kStride];                                     \
     W.x2 ^= ez[(6 * (I) + 2) * kStride];                                     \
-  }
-#define TG_IS_MOVE(I)                                                        \
-  {                                                                          \
-    TG_IS_MOVE_W(I)                                                          \
     Pz.x0 ^= ez[(6 * (I) + 3) * kStride];                                    \
     Pz.x1 ^= ez[(6 * (I) + 4) * kStride];                                    \
     Pz.x2 ^= ez[(6 * (I) + 5) * kStride];                                    \
@@ -852,8 +845,7 @@ __device__ __forceinline__ unsigned long long is_walk_blocks(
       d.x1 ^= ez[37 * kStride];
       d.x2 ^= ez[38 * kStride];
       pl3_xor(W, pl3_mul(d, h));
-      // Pz is at digit 1 = alpha^0 at both block starts: digits 2.. only
-      pl3_xor(Pz, pl3_and(pl3_lo(nx), gz));
+      pl3_xor(Pz, pl3_and(d, gz));
       qh0 ^= nx.h0;
       qh1 ^= nx.h1;
       qh2 ^= nx.h2;
@@ -871,33 +863,19 @@ __device__ __forceinline__ unsigned long long is_walk_blocks(
     // exactly after the block.
     // The pair test pays once thr >= kIsPairThr: below it a pair's count
     // passes thr so often that the exact path costs more than it saves.
-    // Pz is kept at the block's start (digit 1 at alpha^0); the single test
-    // moves a copy of it sweep by sweep, the pair test rebuilds it for a
-    // flagged block only.
     unsigned fl = 0u;
-    Pl3 Pz6 = Pz;
     if (thz + ngz >= kIsPairThr) {
-      TG_IS_SWEEP2(0); TG_IS_MOVE_W(0); TG_IS_SWEEP2(1); TG_IS_MOVE_W(1); TG_IS_SWEEP2(2);
-      TG_IS_MOVE_W(2); TG_IS_SWEEP2(3); TG_IS_MOVE_W(3); TG_IS_SWEEP2(4); TG_IS_MOVE_W(4);
-      TG_IS_SWEEP2(5); TG_IS_MOVE_W(5); TG_IS_SWEEP2(6);
-      if (__builtin_expect(fl != 0u, 0)) {
-#pragma unroll
-        for (int m = 0; m < 6; ++m) {
-          Pz6.x0 ^= ez[(6 * m + 3) * kStride];
-          Pz6.x1 ^= ez[(6 * m + 4) * kStride];
-          Pz6.x2 ^= ez[(6 * m + 5) * kStride];
-        }
-      }
+      TG_IS_SWEEP2(0); TG_IS_MOVE(0); TG_IS_SWEEP2(1); TG_IS_MOVE(1); TG_IS_SWEEP2(2);
+      TG_IS_MOVE(2); TG_IS_SWEEP2(3); TG_IS_MOVE(3); TG_IS_SWEEP2(4); TG_IS_MOVE(4);
+      TG_IS_SWEEP2(5); TG_IS_MOVE(5); TG_IS_SWEEP2(6);
     } else {
-      Pl3 Pz = Pz6;
       TG_IS_SWEEP1(0, 1u); TG_IS_MOVE(0); TG_IS_SWEEP1(1, 2u); TG_IS_MOVE(1); TG_IS_SWEEP1(2, 4u);
       TG_IS_MOVE(2); TG_IS_SWEEP1(3, 3u); TG_IS_MOVE(3); TG_IS_SWEEP1(4, 6u); TG_IS_MOVE(4);
       TG_IS_SWEEP1(5, 7u); TG_IS_MOVE(5); TG_IS_SWEEP1(6, 5u);
-      Pz6 = Pz;
     }
     if (__builtin_expect(fl != 0u, 0)) {
-      wmin = is_block_fix<kStride, kW, kCG>(fl, W, Pz6, ez, ngz, qh0, qh1, qh2, rows + r0,
-                                            rows + r1, wmin, wo, wthr);
+      wmin = is_block_fix<kStride, kW, kCG>(fl, W, Pz, ez, ngz, qh0, qh1, qh2, rows + r0, rows + r1,
+                                       wmin, wo, wthr);
       thz = thz_base - wmin;
     }
     if (wmin < wthr) break;
@@ -909,7 +887,6 @@ __device__ __forceinline__ unsigned long long is_walk_blocks(
 }
 
 #undef TG_IS_MOVE
-#undef TG_IS_MOVE_W
 #undef TG_IS_SWEEP2
 #undef TG_IS_SWEEP1
 #undef TG_IS_ZCOUNTS
