@@ -19,6 +19,7 @@ namespace tg {
 constexpr int kSrvMaxK = kMaxExactK;
 constexpr int kSrvTPB = 128;
 constexpr int kSrvPerSm = 5;  // CTAs per SM: the walk's register and shared-memory budget
+constexpr int kSrvDoorbellStride = 16;  // warp 0 of every 16th CTA reads host memory
 
 enum : unsigned int { kSlotFree = 0, kSlotPrep = 1, kSlotRun = 2, kSlotWait = 3, kSlotDone = 4 };
 
@@ -54,16 +55,27 @@ struct SrvResult {
   uint64_t t_done_ns;
 };
 
+// The words every warp polls or updates sit on cache lines of their own, so
+// the claims and pops of busy warps do not queue behind the reads of idle
+// ones.
+struct alignas(128) SrvLine32 {
+  unsigned int v;
+  unsigned int pad[31];
+};
+struct alignas(128) SrvLine64 {
+  unsigned long long v;
+  unsigned long long pad[15];
+};
+
 struct SrvDevHeader {
-  unsigned int prep_next;             // next published request to prepare
-  unsigned int pub_mirror;            // device copy of SrvCtl::published
-  unsigned long long last_activity;   // globaltimer of the last useful step
+  SrvLine32 prep_next;                // next published request to prepare
+  SrvLine32 pub_mirror;               // device copy of SrvCtl::published
+  SrvLine64 last_activity;            // globaltimer of the last useful step
+  SrvLine32 job_head;                 // next job to serve
+  SrvLine32 job_tail;                 // next free job position
+  SrvLine32 stop_mirror;              // device copy of SrvCtl::stop
   int status;
   unsigned int launches;
-  unsigned int job_head;              // next job to serve
-  unsigned int job_tail;              // next free job position
-  unsigned int stop_mirror;           // device copy of SrvCtl::stop
-  unsigned int pad0;
   unsigned long long tasks_done;
   unsigned long long codewords;       // codewords evaluated (levels 1-3 and the level tasks)
   unsigned long long dedup_hits;

@@ -110,7 +110,7 @@ __device__ __forceinline__ unsigned long long srv_task_units(unsigned long long 
 // Appends a job: level w >= 4 of request gen in `slot`, or (w = 0) the
 // request waiting there on an equivalent one.
 __device__ void srv_push_job(const SrvArgs& a, unsigned int gen, int w, unsigned int slot) {
-  const unsigned int pos = atomicAdd(&a.dh->job_tail, 1u);
+  const unsigned int pos = atomicAdd(&a.dh->job_tail.v, 1u);
   const unsigned long long e = (static_cast<unsigned long long>(gen) << 32) |
                                (static_cast<unsigned long long>(w) << 24) | slot;
   atomicExch(a.jobs + (pos & (a.J - 1u)), e);
@@ -369,7 +369,8 @@ __device__ void srv_resolve(const SrvArgs& a, int lane, unsigned int slot, uint8
 // slot that no longer serves gen, or past the level's end, runs nothing.
 // The warp that counts a level's last task ends the level.
 __device__ void srv_run(const SrvArgs& a, int lane, unsigned int slot, unsigned long long cw,
-                        const unsigned long long (*bn)[kIsBinom], uint16_t* dig, uint32_t* ez) {
+                        const unsigned long long (*bn)[kIsBinom], uint16_t* dig, uint32_t* ez,
+                        unsigned long long& n_tasks, unsigned long long& n_codewords) {
   SrvSlotHdr* h = srv_slot(a, slot);
   const unsigned int gen = static_cast<unsigned int>(cw >> 32);
   const int w = static_cast<int>((cw >> 27) & 31ull);
@@ -396,7 +397,7 @@ __device__ void srv_run(const SrvArgs& a, int lane, unsigned int slot, unsigned 
   const int wl = __reduce_min_sync(0xffffffffu, wmin);
   for (int o = 16; o > 0; o >>= 1) ncw += __shfl_xor_sync(0xffffffffu, ncw, o);
   if (lane == 0) {
-    atomicAdd(&a.dh->codewords, ncw);
+    n_codewords += ncw;  // this warp's statistics, flushed by the loop
     unsigned long long skipped = 0ull;
     if (wl < ld_flag(&h->best)) {
       const int best = min(atomicMin(&h->best, wl), wl);
@@ -413,11 +414,18 @@ __device__ void srv_run(const SrvArgs& a, int lane, unsigned int slot, unsigned 
     __threadfence();
     const unsigned long long add = owned + skipped;
     const unsigned long long old = atomicAdd(&h->done, add);
-    atomicAdd(&a.dh->tasks_done, owned);
+    n_tasks += owned;
     if ((old >> 40) == static_cast<unsigned long long>(w) && (old & kSrvDoneMask) + add == nt)
       srv_level_end(a, slot, h, gen, w);
   }
   __syncwarp();
+}
+
+// Records activity for the idle exit: the shared word is written only when
+// it is more than 50 us old, so busy warps do not queue on it.
+__device__ __forceinline__ void srv_touch(const SrvArgs& a) {
+  const unsigned long long now = gtimer();
+  if (now > ld_vol64(&a.dh->last_activity.v) + 50000ull) atomicMax(&a.dh->last_activity.v, now);
 }
 
 __global__ void __launch_bounds__(kSrvTPB, kSrvPerSm) serve_kernel(SrvArgs a) {
@@ -434,31 +442,37 @@ __global__ void __launch_bounds__(kSrvTPB, kSrvPerSm) serve_kernel(SrvArgs a) {
   uint32_t* my_ez = &s_ez[0][threadIdx.x];
   const unsigned long long t_start = gtimer();
   if (threadIdx.x == 0 && blockIdx.x == 0) {
-    atomicMax(&a.dh->last_activity, t_start);
+    atomicMax(&a.dh->last_activity.v, t_start);
     atomicAdd(&a.dh->launches, 1u);
   }
   unsigned int iter = 0u;
   bool was_idle = true;
+  // Host memory is read over the bus by a few doorbell warps (warp 0 of
+  // every kSrvDoorbellStride-th CTA) when idle or once in 64 steps, and by
+  // every other warp once in 1024 steps; all of them keep to the device
+  // mirrors otherwise.
+  const bool doorbell = wl == 0 && (blockIdx.x % kSrvDoorbellStride) == 0;
+  unsigned long long n_tasks = 0ull, n_codewords = 0ull;  // lane 0's, flushed now and then
   for (;;) {
     int action = 0;  // -1 exit, 0 idle, 1 prepare, 2 run, 3 resolve
     unsigned int arg = 0u, slot = 0u;
     unsigned long long cw = 0ull;
     if (lane == 0) {
-      // Host memory is read over the bus: only an idle warp, or every warp
-      // once in 64 steps, refreshes the device mirrors of the host's counters.
-      if (was_idle || (++iter & 63u) == 0u) {
-        atomicMax(&a.dh->pub_mirror, ld_acquire_sys(&a.ctl->published));
-        if (ld_acquire_sys(&a.ctl->stop)) atomicExch(&a.dh->stop_mirror, 1u);
+      ++iter;
+      if (doorbell ? (was_idle || (iter & 63u) == 0u) : (iter & 1023u) == 0u) {
+        const unsigned int pub = ld_acquire_sys(&a.ctl->published);
+        if (pub > ld_vol32(&a.dh->pub_mirror.v)) atomicMax(&a.dh->pub_mirror.v, pub);
+        if (ld_acquire_sys(&a.ctl->stop)) atomicExch(&a.dh->stop_mirror.v, 1u);
         atomicAdd(&a.dh->host_reads, 1ull);
       }
       const unsigned long long now = gtimer();
-      if (ld_vol32(&a.dh->stop_mirror) || now - t_start > a.life_ns) {
+      if (ld_vol32(&a.dh->stop_mirror.v) || now - t_start > a.life_ns) {
         action = -1;
       } else {
-        const unsigned int pub = ld_vol32(&a.dh->pub_mirror);
-        unsigned int p = ld_vol32(&a.dh->prep_next);
+        const unsigned int pub = ld_vol32(&a.dh->pub_mirror.v);
+        unsigned int p = ld_vol32(&a.dh->prep_next.v);
         while (p < pub) {
-          const unsigned int prev = atomicCAS(&a.dh->prep_next, p, p + 1u);
+          const unsigned int prev = atomicCAS(&a.dh->prep_next.v, p, p + 1u);
           if (prev == p) {
             action = 1;
             arg = p;
@@ -469,8 +483,8 @@ __global__ void __launch_bounds__(kSrvTPB, kSrvPerSm) serve_kernel(SrvArgs a) {
         // The job at the head of the ring: claim from it, or pop it.  A few
         // tries per step keep the warp from looping on a busy ring.
         for (int tries = 0; action == 0 && tries < 8; ++tries) {
-          const unsigned int hd = ld_vol32(&a.dh->job_head);
-          if (hd == ld_vol32(&a.dh->job_tail)) break;
+          const unsigned int hd = ld_vol32(&a.dh->job_head.v);
+          if (hd == ld_vol32(&a.dh->job_tail.v)) break;
           unsigned long long* je = a.jobs + (hd & (a.J - 1u));
           const unsigned long long e = ld_vol64(je);
           if (e == 0ull) break;  // pushed but not yet written
@@ -481,7 +495,7 @@ __global__ void __launch_bounds__(kSrvTPB, kSrvPerSm) serve_kernel(SrvArgs a) {
           if (w == 0) {
             // a waiting request: take the job; resolve it once its
             // equivalent's answer is final, else put it back behind the rest
-            if (atomicCAS(&a.dh->job_head, hd, hd + 1u) != hd) continue;
+            if (atomicCAS(&a.dh->job_head.v, hd, hd + 1u) != hd) continue;
             atomicExch(je, 0ull);
             if (ld_vol32(&h->id) != gen || ld_vol32(&h->state) != kSlotWait) continue;
             const unsigned long long v = ld_vol64(a.vals + __ldcg(&h->tslot));
@@ -513,17 +527,22 @@ __global__ void __launch_bounds__(kSrvTPB, kSrvPerSm) serve_kernel(SrvArgs a) {
             cw = atomicAdd(&h->claim, 32ull);
             action = 2;
             slot = sl;
-          } else if (atomicCAS(&a.dh->job_head, hd, hd + 1u) == hd) {
+          } else if (atomicCAS(&a.dh->job_head.v, hd, hd + 1u) == hd) {
             atomicExch(je, 0ull);
           }
         }
         if (action == 0) {
-          const unsigned long long act = max(ld_vol64(&a.dh->last_activity), t_start);
+          const unsigned long long act = max(ld_vol64(&a.dh->last_activity.v), t_start);
           if (now > act + a.idle_ns) action = -1;
         }
       }
     }
     action = __shfl_sync(0xffffffffu, action, 0);
+    if (lane == 0 && (action < 0 || (iter & 63u) == 0u) && (n_tasks | n_codewords)) {
+      atomicAdd(&a.dh->tasks_done, n_tasks);
+      atomicAdd(&a.dh->codewords, n_codewords);
+      n_tasks = n_codewords = 0ull;
+    }
     if (action < 0) break;
     was_idle = action == 0;
     if (action == 0) {
@@ -534,11 +553,11 @@ __global__ void __launch_bounds__(kSrvTPB, kSrvPerSm) serve_kernel(SrvArgs a) {
     slot = __shfl_sync(0xffffffffu, slot, 0);
     cw = __shfl_sync(0xffffffffu, cw, 0);
     __syncwarp();  // order every lane's loads after lane 0's acquire
-    if (lane == 0) atomicMax(&a.dh->last_activity, gtimer());
+    if (lane == 0) srv_touch(a);
     if (action == 1) srv_prepare(a, lane, arg, s_ord[wl]);
-    else if (action == 2) srv_run(a, lane, slot, cw, s_binom, my_dig, my_ez);
+    else if (action == 2) srv_run(a, lane, slot, cw, s_binom, my_dig, my_ez, n_tasks, n_codewords);
     else srv_resolve(a, lane, slot, s_ord[wl]);
-    if (lane == 0) atomicMax(&a.dh->last_activity, gtimer());
+    if (lane == 0) srv_touch(a);
   }
 }
 
