@@ -523,10 +523,13 @@ __device__ __forceinline__ WitOut wit_out(const DistArgs& a, int c, int j) {
 // 0..31 in the lo words, 32..48 in bits 0..16 of the hi words), as the code's
 // witness in the original column order: the set's non-pivot columns first
 // (increasing), then its pivots, as prep_infoset_kernel ordered them.  Only
-// the first caller per code writes, so the row is never torn.
+// the first caller per code writes, so the row is never torn; its claim word
+// takes the codeword's weight + 1, the value the pass reports (lanes of other
+// warps may meet lighter codewords in the same round).
 __device__ __noinline__ void is_put_witness(WitOut wo, uint32_t l0, uint32_t l1, uint32_t l2,
                                             uint32_t h0, uint32_t h1, uint32_t h2) {
-  if (atomicCAS(wo.lock, 0, 1) != 0) return;
+  const int wt = __popc(l0 | l1 | l2) + __popc((h0 | h1 | h2) & kHiMask);
+  if (atomicCAS(wo.lock, 0, wt + 1) != 0) return;
   const uint64_t piv = *wo.piv & kMask49;
   const uint64_t q0 = uint64_t(l0) | (uint64_t(h0 & kHiMask) << 32);
   const uint64_t q1 = uint64_t(l1) | (uint64_t(h1 & kHiMask) << 32);
@@ -1192,18 +1195,20 @@ __global__ void witness_targets_kernel(const int32_t* out, const int64_t* off, i
   td[c] = off[c + 1] > off[c] ? kN + 1 - m : 1;
 }
 
-// After the witness pass: its values (the zeros of the recorded witnesses)
-// become the results; a code evaluated by the walk without a witness raises
-// TG_ERR_STATE, and any status of the pass is copied into the first pass's
-// header hdr1 (the one tg_distance_status reads).
+// After the witness pass: the zeros of each recorded witness (its claim word
+// holds weight + 1) become the results, the pass's values elsewhere (codes
+// decided without a walk); a code evaluated by the walk without a witness
+// raises TG_ERR_STATE, and any status of the pass is copied into the first
+// pass's header hdr1 (the one tg_distance_status reads).
 __global__ void witness_finish_kernel(DistArgs a2, int32_t* out, WsHeader* hdr1) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= a2.n) return;
   const CodeDesc d = a2.desc[c];
-  if ((d.flags & kIsCodeFlag) != 0 && (d.flags & kDecidedFlag) == 0 && a2.wit_lock[c] == 0)
+  const int lock = a2.wit_lock[c];
+  if ((d.flags & kIsCodeFlag) != 0 && (d.flags & kDecidedFlag) == 0 && lock == 0)
     report_status(hdr1, TG_ERR_STATE);
   if (c == 0 && a2.hdr->status != TG_OK) report_status(hdr1, a2.hdr->status);
-  out[c] = a2.out[c];
+  out[c] = lock != 0 ? kN - (lock - 1) : a2.out[c];
 }
 
 }  // namespace tg
