@@ -45,6 +45,12 @@ POPC_PER_CODEWORD = 14.0 / 8.0  # histogram walk: 7 bins x 2 words per 8 codewor
 # single-count test; where the threshold allows, the kernel tests pairs of
 # codewords with 4 + 1 counts, so the executed POPC can be lower)
 POPC_PER_CODEWORD_INFOSET = 8.0 / 7.0
+# DRAM traffic of one walk_level_kernel launch (dram__bytes_read.sum +
+# dram__bytes_write.sum) from the ncu capture summarised in
+# profiles/walk_level_kernel_infoset_mixed_k.md: level 5 of 1000 sets of k = 14.
+# The walk reads each set's tables (7 x 32 B per row) and the task offsets;
+# it is integer-issue bound, and DRAM stays near idle.
+WALK_LEVEL5_DRAM_BYTES = 2.54e6
 
 
 # --enumeration: (TG_ENUM_* value, description)
@@ -966,7 +972,9 @@ def run_b200_arm(args, d: Dist) -> None:
             "gpu_launches": launches_per_step(kmax, args.enumeration) * args.steps,
             "roofline": {"bound": "int (POPC pipe)", "achieved": achieved / 1e12,
                          "peak": peak / 1e12, "unit": "Tpopc/s", "frac": achieved / peak,
-                         "traffic": None, "kernel": dominant["kernel"],
+                         "traffic": WALK_LEVEL5_DRAM_BYTES,
+                         "traffic_unit": "bytes per level-5 launch (ncu, 1000 sets of k = 14)",
+                         "kernel": dominant["kernel"],
                          "kernel_share": dominant["seconds"] / (statistics.mean(step_ms) / 1e3),
                          "note": dominant["note"] + "; peak = measured POPC/clk/SM x SMs x "
                                  "median SM MHz in the timed region"},
