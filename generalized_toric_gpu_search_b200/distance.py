@@ -356,10 +356,13 @@ class DistanceOracleCUDABP:
         self._lock = threading.Lock()
         self._stage = PinnedBatchStage()
 
-    def _runner_for(self, k_max: int, sampled: bool) -> DistanceRunner:
-        """Launch shape: the fixed config, else the autotuned one for k_max."""
+    def _runner_for(self, k_max: int, early_exit: bool) -> DistanceRunner:
+        """Launch shape: the fixed config, else the autotuned one for k_max.
+        The table is tuned on exact batches (every level walked); a sampled
+        batch, or one whose thresholds can end sets early, keeps the library
+        defaults, whose smaller tasks notice an early exit sooner."""
         cfg = self._fixed
-        if cfg is None and not sampled and self._table:
+        if cfg is None and not early_exit and self._table:
             from .autotune import choose
 
             cfg = choose(self._table, k_max)
@@ -422,7 +425,9 @@ class DistanceOracleCUDABP:
                     d_td = torch.from_numpy(td_arr).to(self.device)
                 d_out = torch.empty(n, dtype=torch.int32, device=self.device)
                 d_wit = torch.empty((n, N_POINTS), dtype=torch.uint8, device=self.device)
-                runner = self._runner_for(k_max, False)
+                runner = self._runner_for(
+                    k_max, not per_set_td and int(target_distance) > 1 or
+                    per_set_td and bool((np.asarray(target_distance) > 1).any()))
                 p = runner.params(n, k_max, 0 if per_set_td else int(target_distance))
                 runner.run_witness(p, d_idx, d_off, d_out, d_wit, d_target=d_td, stream=s)
                 h_out = d_out.to("cpu", non_blocking=True)
@@ -470,7 +475,9 @@ class DistanceOracleCUDABP:
                 if td_arr is not None:
                     d_td = torch.from_numpy(td_arr).pin_memory().to(self.device, non_blocking=True)
                 d_out = torch.empty(n, dtype=torch.int32, device=self.device)
-                self.runner = self._runner_for(k_max, sample_count > 0)
+                early = sample_count > 0 or (
+                    bool((td_arr > 1).any()) if td_arr is not None else int(target_distance) > 1)
+                self.runner = self._runner_for(k_max, early)
                 p = self.runner.params(n, k_max, 0 if per_set_td else int(target_distance),
                                        sample_count if sample_count > 0 else 0, sample_seed)
                 self.runner.run(p, d_idx, d_off, d_out, d_target=d_td, stream=s)
