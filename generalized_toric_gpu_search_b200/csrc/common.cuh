@@ -200,25 +200,25 @@ __device__ __forceinline__ uint64_t canon_mask_warp_min(int lane, uint64_t S,
       img |= 1ull << idx;
       R |= 1u << ((idx * 37) >> 8);  // row idx / 7
     }
-    uint64_t y = img;
-    while (y) {
-      const int q = __ffsll(static_cast<long long>(y)) - 1;
-      y &= y - 1ull;
-      const int qa = (q * 37) >> 8;  // q / 7 for q < 49
-      const int qb = q - 7 * qa;
+    // Anchors q = (qa, qb) row by row: the rows after the shift, and so the
+    // top row t and the image row ra that lands on it, depend on qa only.
+    for (uint32_t rows = R; rows != 0u; rows &= rows - 1u) {
+      const int qa = __ffs(rows) - 1;
       const uint32_t rr = ((R >> qa) | (R << (7 - qa))) & 0x7Fu;  // rows after the shift
       const int t = 31 - __clz(rr);
       if (t > tb) continue;
-      if (t == tb) {
-        int ra = qa + t;
-        ra = ra >= 7 ? ra - 7 : ra;
-        const uint32_t rb = uint32_t(img >> (7 * ra)) & 0x7Fu;
-        if ((((rb >> qb) | (rb << (7 - qb))) & 0x7Fu) > pb) continue;
-      }
-      const uint64_t cand = torus_shift(img, qa, qb);
-      if (cand < best) {
-        best = cand;
-        mask_top_row(best, tb, pb);
+      int ra = qa + t;
+      ra = ra >= 7 ? ra - 7 : ra;
+      const uint32_t rb = uint32_t(img >> (7 * ra)) & 0x7Fu;
+      for (uint32_t cols = uint32_t(img >> (7 * qa)) & 0x7Fu; cols != 0u; cols &= cols - 1u) {
+        const int qb = __ffs(cols) - 1;
+        // t <= tb here; an improvement makes tb = t
+        if (t == tb && (((rb >> qb) | (rb << (7 - qb))) & 0x7Fu) > pb) continue;
+        const uint64_t cand = torus_shift(img, qa, qb);
+        if (cand < best) {
+          best = cand;
+          mask_top_row(best, tb, pb);
+        }
       }
     }
     if ((it & 7) == 7 || A + 32 >= kGl2Order) {  // every lane runs 63 matrices
