@@ -63,12 +63,29 @@ ENUMERATIONS = {
 }
 
 
+def last_infoset_level(k_max: int) -> int:
+    """The last level the information-set walk launches for the toric matrix
+    (tg_infoset_last_level): the smallest L with ceil(49 (L + 1) / k) above
+    the Griesmer cap of a [49, k] code over GF(8), maximised over k <= k_max."""
+    import math
+
+    last = 0
+    for k in range(1, k_max + 1):
+        cap = max(d for d in range(1, 50)
+                  if sum(math.ceil(d / 8 ** i) for i in range(k)) <= 49)
+        L = 0
+        while math.ceil(49 * (L + 1) / k) < cap + 1:
+            L += 1
+        last = max(last, min(L, k))
+    return last
+
+
 def launches_per_step(k_max: int, enumeration: str) -> int:
     """Kernels per step: prep_exact, scan_tasks and the enumeration walk; with
     information sets also prep_infoset, levels123 (levels 1 to 3), per level
-    4..k_max plan, scan and walk, and finalize_infoset."""
+    4..last_infoset_level(k_max) plan, scan and walk, and finalize_infoset."""
     infoset = enumeration == "infoset" or (enumeration == "auto" and k_max >= 2)
-    return 3 + ((3 + 3 * max(0, k_max - 3)) if infoset else 0)
+    return 3 + ((3 + 3 * max(0, last_infoset_level(k_max) - 3)) if infoset else 0)
 
 
 L2_FLUSH_BYTES = 256 << 20

@@ -64,6 +64,7 @@ SIGNATURES: dict[str, tuple] = {
     "tg_max_zeros_walk_part": (
         c_int, [c_void_p, c_void_p, c_int32, c_void_p, c_void_p, c_size_t, c_void_p]
     ),
+    "tg_infoset_last_level": (c_int, [c_int32, c_int32, POINTER(c_int32)]),
     "tg_witness_workspace_size": (c_int, [c_void_p, POINTER(c_size_t)]),
     "tg_max_zeros_witness": (
         c_int,

@@ -412,6 +412,13 @@ static WitLayout witness_layout(const tg_distance_params& p) {
 
 extern "C" {
 
+int tg_infoset_last_level(int32_t k_max, int32_t is_toric, int32_t* h_level) {
+  if (!h_level) return invalid("tg_infoset_last_level: NULL output");
+  if (k_max < 0 || k_max > kMaxExactK) return invalid("k_max must be 0..21");
+  *h_level = infoset_last_level(k_max, is_toric ? 1 : 0);
+  return TG_OK;
+}
+
 int tg_witness_workspace_size(const tg_distance_params* p, size_t* h_bytes) {
   int st = check_distance_params(p);
   if (st) return st;

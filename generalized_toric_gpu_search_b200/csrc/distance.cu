@@ -852,6 +852,34 @@ static cudaError_t launch_walk(int variant, bool sampled, int grid, int blocks_p
   return cudaGetLastError();
 }
 
+// Last level the information-set walk can need for a batch whose sets have
+// at most k_max rows.  With the toric matrix, after levels 1..L every unseen
+// codeword of a k-row code weighs at least ceil(49 (L + 1) / k); the Griesmer
+// bound n >= sum_{i < k} ceil(d / 8^i) caps the distance d of any [49, k]
+// code over GF(8) at some G(k).  Once ceil(49 (L + 1) / k) > G(k) a
+// minimum-weight codeword has been met and plan_level_kernel stops the code,
+// so no level after that L is needed by any k <= k_max.  Other matrices use
+// the disjoint-set bound: every level up to k_max.
+int infoset_last_level(int k_max, int is_toric) {
+  if (!is_toric) return k_max;
+  int last = 0;
+  for (int k = 1; k <= k_max; ++k) {
+    int G = 0;
+    for (int d = 1; d <= kN; ++d) {
+      long long sum = 0, q = 1;
+      for (int i = 0; i < k && sum <= kN; ++i) {
+        sum += (d + q - 1) / q;
+        if (q < (1ll << 40)) q *= 8;
+      }
+      if (sum <= kN) G = d;
+    }
+    int L = 0;
+    while ((kN * (L + 1) + k - 1) / k < G + 1) ++L;
+    last = std::max(last, std::min(L, k));
+  }
+  return last;
+}
+
 int run_prepare(const DistArgs& args, cudaStream_t s) {
   if (args.n <= 0) return TG_OK;
   const bool sampled = args.sample_count > 0;
@@ -901,7 +929,8 @@ int run_walk(const DistArgs& args, int sm_count, int blocks_per_sm, int tpb, cud
     la.is_lanes = sm_count * per_sm * kIsWalkThreads;
     const int plan_grid = (args.n + 255) / 256;
     levels123_kernel<<<(args.n + 3) / 4, 128, 0, s>>>(la);
-    for (int w = 4; w <= args.k_max; ++w) {
+    const int w_last = infoset_last_level(args.k_max, args.is_toric);
+    for (int w = 4; w <= w_last; ++w) {
       plan_level_kernel<<<plan_grid, 256, 0, s>>>(la, w);
       scan_level_kernel<<<1, kScanThreads, 0, s>>>(la, w);
       if (la.witness)

@@ -123,6 +123,7 @@ int default_tail_rows(const tg_distance_params& p);
 int infoset_min_k(const tg_distance_params& p);
 WsLayout ws_layout(const tg_distance_params& p);
 int run_prepare(const DistArgs& args, cudaStream_t s);
+int infoset_last_level(int k_max, int is_toric);
 // parts: kWalkEnumeration (orbit / projective / sampled walk) and/or
 // kWalkInfoset (information-set walk and its finalisation).
 constexpr int kWalkEnumeration = 1;

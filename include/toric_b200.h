@@ -176,6 +176,14 @@ int tg_max_zeros_walk_part(tg_context* ctx, const tg_distance_params* p,
                            int32_t parts, int32_t* d_out, void* d_workspace,
                            size_t workspace_bytes, void* stream);
 
+/* Last information-set level a batch with sets of at most k_max rows can
+ * need (levels 1..3 always run; levels 4..*h_level are launched).  For the
+ * toric matrix: the smallest L with ceil(49 (L + 1) / k) above the Griesmer
+ * cap of a [49, k] code over GF(8), maximised over k <= k_max (9 for
+ * k_max = 14); for other matrices k_max.  No
+ * counterpart in the reference, which walks every message.  Needs no GPU. */
+int tg_infoset_last_level(int32_t k_max, int32_t is_toric, int32_t* h_level);
+
 /* Bytes of workspace tg_max_zeros_witness needs (exact parameters only). */
 int tg_witness_workspace_size(const tg_distance_params* p, size_t* h_bytes);
 

@@ -111,3 +111,23 @@ def test_context_without_device(lib):
     assert st == _lib.TG_ERR_NO_DEVICE
     with pytest.raises(RuntimeError, match="No CUDA GPU found"):
         _lib.check(st, "tg_context_create")
+
+
+def test_infoset_last_level_matches_the_griesmer_cap():
+    """The information-set walk's level cap (tg_infoset_last_level) against a
+    Python restatement: after level L a k-row toric code's unseen codewords
+    weigh >= ceil(49 (L + 1) / k); the Griesmer bound caps d of a [49, k]
+    code over GF(8)."""
+    import bench
+
+    lib_build.build()
+    lib = _lib.load()
+    out = ctypes.c_int32(0)
+    for k_max in range(0, 22):
+        assert lib.tg_infoset_last_level(k_max, 1, ctypes.byref(out)) == 0
+        assert out.value == bench.last_infoset_level(k_max)
+        assert lib.tg_infoset_last_level(k_max, 0, ctypes.byref(out)) == 0
+        assert out.value == k_max
+    lib.tg_infoset_last_level(14, 1, ctypes.byref(out))
+    assert out.value == 9
+    assert lib.tg_infoset_last_level(22, 1, ctypes.byref(out)) == _lib.TG_ERR_INVALID_ARGUMENT
