@@ -23,8 +23,9 @@
 
 namespace tg {
 
-constexpr int kCanonTPB = 256;
-constexpr int kGl2Bytes = kGl2Order * kN;          // 98,784
+constexpr int kCanonTPB = 512;                     // 2 CTAs per SM: 32 warps
+constexpr int kGl2Row = 52;                        // padded row in shared memory
+constexpr int kGl2SharedBytes = kGl2Order * kGl2Row;  // 104,832
 
 struct CanonArgs {
   const int32_t* sets;    // (n, k) rows, or NULL
@@ -41,10 +42,10 @@ struct CanonArgs {
 
 __global__ void __launch_bounds__(kCanonTPB, 2) canon_kernel(CanonArgs a) {
   extern __shared__ __align__(16) uint8_t s_perm[];
-  {
-    const uint4* src = reinterpret_cast<const uint4*>(a.gl2);
-    uint4* dst = reinterpret_cast<uint4*>(s_perm);
-    for (int i = threadIdx.x; i < kGl2Bytes / 16; i += blockDim.x) dst[i] = __ldg(src + i);
+  // the GL2 table, rows padded from 49 to kGl2Row bytes
+  for (int i = threadIdx.x; i < kGl2Order * kN; i += blockDim.x) {
+    const int m = i / kN;
+    s_perm[m * kGl2Row + (i - m * kN)] = __ldg(a.gl2 + i);
   }
   __syncthreads();
   const int lane = threadIdx.x & 31;
@@ -83,7 +84,7 @@ __global__ void __launch_bounds__(kCanonTPB, 2) canon_kernel(CanonArgs a) {
       }
       continue;
     }
-    const uint64_t best = canon_mask_warp_min<false>(lane, S, s_perm);
+    const uint64_t best = canon_mask_warp_min<false, kGl2Row>(lane, S, s_perm);
     if (lane == 0) {
       a.out_mask[s] = best;
       uint64_t lo, hi;
@@ -103,7 +104,7 @@ int run_canonical(int device, int sm_count, const uint8_t* d_gl2, const int32_t*
   if (n <= 0) return TG_OK;
   if (!g_canon_attr[device]) {
     cudaError_t e = cudaFuncSetAttribute(canon_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         kGl2Bytes);
+                                         kGl2SharedBytes);
     if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(canon_kernel)");
     g_canon_attr[device] = true;
   }
@@ -112,7 +113,7 @@ int run_canonical(int device, int sm_count, const uint8_t* d_gl2, const int32_t*
   int grid = sm_count * 2;
   const int max_grid = (warps_needed + (kCanonTPB / 32) - 1) / (kCanonTPB / 32);
   if (grid > max_grid) grid = max_grid;
-  canon_kernel<<<grid, kCanonTPB, kGl2Bytes, s>>>(a);
+  canon_kernel<<<grid, kCanonTPB, kGl2SharedBytes, s>>>(a);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "canon_kernel launch");
   return TG_OK;

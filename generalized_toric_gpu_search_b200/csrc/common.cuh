@@ -182,14 +182,17 @@ __device__ __forceinline__ void mask_top_row(uint64_t m, int& t, uint32_t& bits)
 // of the image, so candidates above the best so far are skipped without the
 // full translation.  The lanes share their best every 8 matrices.  Returns the
 // mask in every lane.
-template <bool kLdg>
+// kRow: bytes between the table's rows (49 in global memory; the shared copy
+// pads rows to 52 bytes, a 13-word stride that keeps the lanes' loads on
+// distinct banks).
+template <bool kLdg, int kRow = kN>
 __device__ __forceinline__ uint64_t canon_mask_warp_min(int lane, uint64_t S,
                                                          const uint8_t* perm) {
   uint64_t best = ~0ull;
   int tb = 9;           // best's top row (9: none yet)
   uint32_t pb = 0x7Fu;  // best's top-row bits
   for (int A = lane, it = 0; A < kGl2Order; A += 32, ++it) {
-    const uint8_t* P = perm + A * kN;
+    const uint8_t* P = perm + A * kRow;
     uint64_t img = 0ull;
     uint32_t R = 0u;
     uint64_t x = S;
