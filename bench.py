@@ -83,9 +83,10 @@ def last_infoset_level(k_max: int) -> int:
 def launches_per_step(k_max: int, enumeration: str) -> int:
     """Kernels per step: prep_exact, scan_tasks and the enumeration walk; with
     information sets also prep_infoset, levels123 (levels 1 to 3), per level
-    4..last_infoset_level(k_max) plan, scan and walk, and finalize_infoset."""
+    4..last_infoset_level(k_max) two parts of plan, scan and walk each, and
+    finalize_infoset."""
     infoset = enumeration == "infoset" or (enumeration == "auto" and k_max >= 2)
-    return 3 + ((3 + 3 * max(0, last_infoset_level(k_max) - 3)) if infoset else 0)
+    return 3 + ((3 + 6 * max(0, last_infoset_level(k_max) - 3)) if infoset else 0)
 
 
 L2_FLUSH_BYTES = 256 << 20
@@ -934,8 +935,8 @@ def run_b200_arm(args, d: Dist) -> None:
     peak = pipes.get("popc_per_clk_sm", 16.0) * sm_count * (mhz or 1965.0) * 1e6
     enum_s, is_s = statistics.mean(enum_ms) / 1e3, statistics.mean(is_ms) / 1e3
     if is_s >= enum_s:
-        dominant = {"kernel": "walk_level_kernel (one launch per level, with plan_level_kernel, "
-                              "scan_level_kernel and finalize_infoset_kernel)",
+        dominant = {"kernel": "walk_level_kernel (two launches per level, one per part, with "
+                              "plan_level_kernel, scan_level_kernel and finalize_infoset_kernel)",
                     "seconds": is_s, "codewords": paths["infoset_codewords"],
                     "popc_per_codeword": POPC_PER_CODEWORD_INFOSET,
                     "note": "8 POPC per 7 codewords (seven zero-selection counts on the low "

@@ -930,15 +930,19 @@ int run_walk(const DistArgs& args, int sm_count, int blocks_per_sm, int tpb, cud
     const int plan_grid = (args.n + 255) / 256;
     levels123_kernel<<<(args.n + 3) / 4, 128, 0, s>>>(la);
     const int w_last = infoset_last_level(args.k_max, args.is_toric);
+    // Each level in two parts (a toric code's supports with and without its
+    // last row; other codes walk the whole level in part 1).
     for (int w = 4; w <= w_last; ++w) {
-      plan_level_kernel<<<plan_grid, 256, 0, s>>>(la, w);
-      scan_level_kernel<<<1, kScanThreads, 0, s>>>(la, w);
-      if (la.witness)
-        walk_level_kernel<kIsWalkThreads, kPerSm, true>
-            <<<sm_count * per_sm, kIsWalkThreads, 0, s>>>(la, w);
-      else
-        walk_level_kernel<kIsWalkThreads, kPerSm, false>
-            <<<sm_count * per_sm, kIsWalkThreads, 0, s>>>(la, w);
+      for (int part = 1; part <= 2; ++part) {
+        plan_level_kernel<<<plan_grid, 256, 0, s>>>(la, w, part);
+        scan_level_kernel<<<1, kScanThreads, 0, s>>>(la, w);
+        if (la.witness)
+          walk_level_kernel<kIsWalkThreads, kPerSm, true>
+              <<<sm_count * per_sm, kIsWalkThreads, 0, s>>>(la, w, part);
+        else
+          walk_level_kernel<kIsWalkThreads, kPerSm, false>
+              <<<sm_count * per_sm, kIsWalkThreads, 0, s>>>(la, w, part);
+      }
     }
     finalize_infoset_kernel<<<plan_grid, 256, 0, s>>>(la);
     e = cudaGetLastError();

@@ -316,27 +316,72 @@ __device__ __forceinline__ unsigned long long is_max_task_units(int w) {
   return w >= 3 ? 343ull : (w == 2 ? 2401ull : 16807ull);
 }
 
-// Decides, with levels 1..w-1 complete, whether each code is finished, and
-// the units of level w of those that are not.
-__global__ void plan_level_kernel(DistArgs a, int w) {
+// Level w of a toric code runs in two parts.  Part 1 takes the supports that
+// hold the last row (index k - 1): C(k-1, w-1) of them, support ranks
+// C(k-1, w) .. C(k, w) - 1.  Part 2 takes the others: C(k-1, w), ranks
+// 0 .. C(k-1, w) - 1.  Let e be the pivot column of row k - 1.  A codeword c
+// not met by levels 1..w-1 and part 1 weighs at least w on every translate
+// E + t of the information set, and w + 1 on each translate whose
+// restriction of c holds e + t (had it weighed w there, its shift by t
+// would be a part-1 message).  Those are the wt(c) translates with e + t in
+// the support of c, so k wt >= 49 w + wt, i.e.
+//   wt >= ceil(49 w / (k - 1))   after part 1,
+// against ceil(49 w / k) before it and ceil(49 (w + 1) / k) after part 2.
+// Any other code walks its whole level in part 1 and nothing in part 2.
+__device__ __forceinline__ bool is_split_level(int32_t flags) {
+  return (flags & kTorusBoundFlag) != 0;
+}
+
+// Supports of part `part` of level w of a k-row code: their count and the
+// rank of the first.
+__device__ __forceinline__ void is_part_supports(int32_t flags, int k, int w, int part,
+                                                 const unsigned long long (*bn)[kIsBinom],
+                                                 unsigned long long& n_sup,
+                                                 unsigned long long& s_off) {
+  if (!is_split_level(flags)) {
+    n_sup = part == 1 ? bn[k][w] : 0ull;
+    s_off = 0ull;
+  } else if (part == 1) {
+    n_sup = bn[k - 1][w - 1];
+    s_off = bn[k - 1][w];
+  } else {
+    n_sup = bn[k - 1][w];
+    s_off = 0ull;
+  }
+}
+
+// Decides, with everything before part `part` (1 or 2) of level w complete,
+// whether each code is finished, and the units of that part for the others.
+__global__ void plan_level_kernel(DistArgs a, int w, int part) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long units = 0ull;
   const CodeDesc d = c < a.n ? a.desc[c] : CodeDesc{};
   if (c < a.n && (d.flags & kIsCodeFlag) != 0 && (d.flags & kDecidedFlag) == 0 &&
-      a.abort[c] == 0) {
+      a.abort[c] == 0 && (part == 1 || is_split_level(d.flags))) {
     const int best = a.is_best[c];
-    const int L = w - 1;
-    const int bound = (d.flags & kTorusBoundFlag)
-                          ? (kN * (L + 1) + d.k - 1) / d.k
-                          : d.R * (L + 1) + (d.n_pat > 0 ? max(0, L + 1 - d.n_pat) : 0);
-    if (w > d.k || best <= bound || best < kN - d.tmax) {
+    bool done = w > d.k || best < kN - d.tmax;  // every message seen, or a witness
+    if (!done) {
+      int bound;
+      if (!is_split_level(d.flags)) {
+        const int L = w - 1;
+        bound = d.R * (L + 1) + (d.n_pat > 0 ? max(0, L + 1 - d.n_pat) : 0);
+      } else if (part == 1) {
+        bound = (kN * w + d.k - 1) / d.k;
+      } else {
+        bound = (kN * w + d.k - 2) / (d.k - 1);  // w <= k, so k >= 4 here
+      }
+      done = best <= bound;
+    }
+    if (done) {
       a.abort[c] = 1;  // exact (bound met or every message seen), or a witness
     } else {
-      units = static_cast<unsigned long long>(d.H) * c_binom[d.k][w] * is_units_per_support(w);
+      unsigned long long n_sup, s_off;
+      is_part_supports(d.flags, d.k, w, part, c_binom, n_sup, s_off);
+      units = static_cast<unsigned long long>(d.H) * n_sup * is_units_per_support(w);
     }
   }
   if (c < a.n) a.is_units[c] = units;
-  // Lets scan_level_kernel and walk_level_kernel skip a level no set needs.
+  // Lets scan_level_kernel and walk_level_kernel skip a part no set needs.
   if (__any_sync(0xffffffffu, units != 0ull) && (threadIdx.x & 31) == 0) a.is_hdr->work = 1;
 }
 
@@ -906,8 +951,9 @@ struct WitSrc {
   int32_t* lock;
 };
 
-// Units [u0, u1) of level w of one code whose information sets start at
-// `base` (n_sets sets of k rows, the last with rank deficit delta); `stop`
+// Units [u0, u1) of one part of level w of one code whose information sets
+// start at `base` (n_sets sets of k rows, the last with rank deficit delta):
+// per set, the n_sup supports of ranks s_off .. s_off + n_sup - 1.  `stop`
 // is the code's abort flag.  The smallest weight met (or wmin when none is
 // smaller), and the codewords evaluated in ncw.  dig and ez (stride kStride)
 // are this thread's shared scratch: the rows of digits 2..w-2 and digit 1's
@@ -917,9 +963,9 @@ __device__ __forceinline__ int is_walk_range(const V6* base, int n_sets, int del
                                              const int32_t* stop, WitSrc wsrc,
                                              const unsigned long long (*bn)[kIsBinom],
                                              uint16_t* dig, uint32_t* ez, int k, int w,
+                                             unsigned long long n_sup, unsigned long long s_off,
                                              unsigned long long u0, unsigned long long u1,
                                              int wthr, int wmin, unsigned long long& ncw) {
-  const unsigned long long n_sup = bn[k][w];
   const unsigned long long bps = is_units_per_support(w);
   const unsigned long long per_set = n_sup * bps;
   ncw = 0ull;
@@ -948,7 +994,7 @@ __device__ __forceinline__ int is_walk_range(const V6* base, int n_sets, int del
     V6 P;
     v6_zero(P);
     uint32_t r0 = 0u, r1 = 0u;
-    unsigned long long srank = s, rest = b;
+    unsigned long long srank = s + s_off, rest = b;
     int rem = w, q = 0;
     for (int pos = k - 1; pos >= 0 && rem > 0; --pos) {
       const unsigned long long bb = bn[pos][rem];
@@ -996,19 +1042,23 @@ __device__ __forceinline__ int is_walk_range(const V6* base, int n_sets, int del
   return wmin;
 }
 
-// is_walk_range for code c of a batch.
+// is_walk_range for part `part` of level w of code c of a batch.
 template <int kStride, bool kW>
 __device__ __forceinline__ int is_walk_units(const DistArgs& a,
                                              const unsigned long long (*bn)[kIsBinom],
                                              uint16_t* dig, uint32_t* ez, int c, int k, int w,
-                                             unsigned long long u0, unsigned long long u1,
-                                             int wthr, int wmin, unsigned long long& ncw) {
+                                             int part, unsigned long long u0,
+                                             unsigned long long u1, int wthr, int wmin,
+                                             unsigned long long& ncw) {
   const WitSrc wsrc = kW ? WitSrc{a.is_piv + size_t(c) * kIsMaxSets, a.witness + size_t(c) * kN,
                                   a.wit_lock + c}
                          : WitSrc{nullptr, nullptr, nullptr};
-  return is_walk_range<kStride, kW, false>(a.is_rows + size_t(c) * a.is_stride, a.desc[c].H,
-                                    a.desc[c].n_pat, a.abort + c, wsrc, bn, dig, ez, k, w, u0,
-                                    u1, wthr, wmin, ncw);
+  const CodeDesc& d = a.desc[c];
+  unsigned long long n_sup, s_off;
+  is_part_supports(d.flags, k, w, part, bn, n_sup, s_off);
+  return is_walk_range<kStride, kW, false>(a.is_rows + size_t(c) * a.is_stride, d.H, d.n_pat,
+                                           a.abort + c, wsrc, bn, dig, ez, k, w, n_sup, s_off,
+                                           u0, u1, wthr, wmin, ncw);
 }
 
 constexpr int kIsMaxDigits = kMaxExactK - 3;  // digits 2..w-2, w <= 21
@@ -1016,7 +1066,8 @@ constexpr int kIsMaxDigits = kMaxExactK - 3;  // digits 2..w-2, w <= 21
 // kW: the witness pass (per-code targets 50 - max_zeros; the first codeword
 // below a target is recorded as that code's witness).
 template <int kTPB, int kMinBlocks, bool kW>
-__global__ void __launch_bounds__(kTPB, kMinBlocks) walk_level_kernel(DistArgs a, int w) {
+__global__ void __launch_bounds__(kTPB, kMinBlocks) walk_level_kernel(DistArgs a, int w,
+                                                                       int part) {
   __shared__ unsigned long long s_binom[kIsBinom][kIsBinom];
   __shared__ uint16_t s_dig[kIsMaxDigits][kTPB];
   __shared__ uint32_t s_ez[39][kTPB];
@@ -1065,8 +1116,8 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) walk_level_kernel(DistArgs a
         unsigned long long ncw = 0ull;
         // Codewords no lighter than the code's best so far cannot change it,
         // so the walk starts from that best.
-        wmin = is_walk_units<kTPB, kW>(a, s_binom, my_dig, my_ez, c, a.desc[c].k, w, u0, u1,
-                                       kN - a.desc[c].tmax, best0, ncw);
+        wmin = is_walk_units<kTPB, kW>(a, s_binom, my_dig, my_ez, c, a.desc[c].k, w, part, u0,
+                                       u1, kN - a.desc[c].tmax, best0, ncw);
         evaluated += ncw;
       }
     }

@@ -26,10 +26,14 @@ enum : unsigned int { kSlotFree = 0, kSlotPrep = 1, kSlotRun = 2, kSlotWait = 3,
 // Dedup table value: state << 56 | max_zeros << 48 | leader id.
 enum : unsigned int { kEntEmpty = 0, kEntInFlight = 1, kEntExact = 2, kEntAbort = 3 };
 
-// Claim word of a request: id << 32 | level << 27 | next unclaimed task of
-// that level.  Done word: level << 40 | tasks of that level counted.
-constexpr unsigned long long kSrvTaskMask = (1ull << 27) - 1ull;
-constexpr unsigned long long kSrvMaxTasks = (1ull << 27) - (1ull << 20);
+// A request's levels from 4 on run in two parts each (the supports that hold
+// its last row, then the others); stage 2 w + part - 1 (>= 8) names part
+// `part` of level w.  Claim word of a request: id << 32 | stage << 26 | next
+// unclaimed task of that stage.  Done word: stage << 40 | tasks of that stage
+// counted.
+constexpr int kSrvFirstStage = 8;  // level 4, part 1
+constexpr unsigned long long kSrvTaskMask = (1ull << 26) - 1ull;
+constexpr unsigned long long kSrvMaxTasks = (1ull << 26) - (1ull << 20);
 constexpr unsigned long long kSrvDoneMask = (1ull << 40) - 1ull;
 
 struct SrvCtl {
@@ -80,7 +84,7 @@ struct SrvDevHeader {
   unsigned long long codewords;       // codewords evaluated (levels 1-3 and the level tasks)
   unsigned long long dedup_hits;
   unsigned long long finished;
-  unsigned long long levels_opened;   // level jobs pushed
+  unsigned long long levels_opened;   // stage jobs pushed (two per level)
   unsigned long long wait_requeues;   // wait jobs put back behind the others
   unsigned long long host_reads;      // refreshes of the mirrors from host memory
 };
@@ -92,7 +96,7 @@ struct SrvSlotHdr {
   int best;    // smallest weight met (levels done and tasks counted); 64 = none
   int abort;   // a weight below the target distance was met
   int leader;
-  int level;   // level whose tasks are out
+  int level;   // stage whose tasks are out
   unsigned long long claim;
   unsigned long long done;
   unsigned long long tslot;  // dedup table slot or ~0
@@ -109,7 +113,7 @@ struct SrvArgs {
   uint8_t* slots;
   size_t slot_bytes;
   size_t rows_off;            // the information set within a slot
-  unsigned long long* jobs;   // job ring: id << 32 | level << 24 | slot (0 = empty)
+  unsigned long long* jobs;   // job ring: id << 32 | stage << 24 | slot (0 = empty)
   unsigned int J;             // job ring capacity (power of two)
   unsigned long long* keys;
   unsigned long long* vals;

@@ -6,10 +6,13 @@
 // mask and looks it up in the dedup table, then eliminates its k rows to one
 // information set, walks levels 1 to 3 itself and, while the torus-orbit
 // bound ceil(49 (L + 1) / k) stays below its best weight, opens level 4.
-// Every level of every request is a job in one device ring; warps take 32
-// tasks at a time from the oldest job, so the levels of requests admitted at
-// different times share the SMs (continuous batching).  The warp that counts
-// a level's last task settles the request or opens its next level.
+// Levels from 4 on run in two parts, as in the batch walk: the supports that
+// hold the last row, after which the bound is ceil(49 w / (k - 1)), then the
+// others.  Every part (stage) of every request is a job in one device ring;
+// warps take 32 tasks at a time from the oldest job, so the stages of
+// requests admitted at different times share the SMs (continuous batching).
+// The warp that counts a stage's last task settles the request or opens its
+// next stage.
 //
 // Every warp of the persistent grid loops:
 //   1. prepare the next published request, if any;
@@ -78,10 +81,24 @@ __device__ uint64_t canon_mask_warp(int lane, uint64_t S, const uint8_t* gl2) {
   return canon_mask_warp_min<true>(lane, S, gl2);
 }
 
-// Units of level w of a k-row request (one information set).
+__device__ __forceinline__ int srv_stage(int w, int part) { return 2 * w + part - 1; }
+__device__ __forceinline__ int srv_stage_level(int st) { return st >> 1; }
+__device__ __forceinline__ int srv_stage_part(int st) { return (st & 1) + 1; }
+
+// Supports of stage st of a k-row request (one information set): their count
+// and the rank of the first.
+__device__ __forceinline__ void srv_supports(const unsigned long long (*bn)[kIsBinom], int k,
+                                            int st, unsigned long long& n_sup,
+                                            unsigned long long& s_off) {
+  is_part_supports(kTorusBoundFlag, k, srv_stage_level(st), srv_stage_part(st), bn, n_sup, s_off);
+}
+
+// Units of stage st of a k-row request.
 __device__ __forceinline__ unsigned long long srv_units(const unsigned long long (*bn)[kIsBinom],
-                                                       int k, int w) {
-  return bn[k][w] * is_units_per_support(w);
+                                                       int k, int st) {
+  unsigned long long n_sup, s_off;
+  srv_supports(bn, k, st, n_sup, s_off);
+  return n_sup * is_units_per_support(srv_stage_level(st));
 }
 
 // Units per task of a level: the batch scan's rule for one code (about eight
@@ -107,12 +124,12 @@ __device__ __forceinline__ unsigned long long srv_task_units(unsigned long long 
   return nb;
 }
 
-// Appends a job: level w >= 4 of request gen in `slot`, or (w = 0) the
-// request waiting there on an equivalent one.
-__device__ void srv_push_job(const SrvArgs& a, unsigned int gen, int w, unsigned int slot) {
+// Appends a job: stage st >= kSrvFirstStage of request gen in `slot`, or
+// (st = 0) the request waiting there on an equivalent one.
+__device__ void srv_push_job(const SrvArgs& a, unsigned int gen, int st, unsigned int slot) {
   const unsigned int pos = atomicAdd(&a.dh->job_tail.v, 1u);
   const unsigned long long e = (static_cast<unsigned long long>(gen) << 32) |
-                               (static_cast<unsigned long long>(w) << 24) | slot;
+                               (static_cast<unsigned long long>(st) << 24) | slot;
   atomicExch(a.jobs + (pos & (a.J - 1u)), e);
 }
 
@@ -150,24 +167,27 @@ __device__ void srv_settle(const SrvArgs& a, unsigned int slot, SrvSlotHdr* h, i
   srv_finish(a, slot, h, m, (witness || m > tmax) ? TG_RESULT_FAIL : TG_RESULT_PASS);
 }
 
-// Opens level w of request gen: its done count, then its claim word (from
-// here on a claim tagged (gen, w) refers to this level), then its job.
+// Opens stage st of request gen: its done count, then its claim word (from
+// here on a claim tagged (gen, st) refers to this stage), then its job.
 __device__ void srv_open_level(const SrvArgs& a, unsigned int slot, SrvSlotHdr* h,
-                               unsigned int gen, int w) {
-  atomicExch(&h->done, static_cast<unsigned long long>(w) << 40);
-  h->level = w;
+                               unsigned int gen, int st) {
+  atomicExch(&h->done, static_cast<unsigned long long>(st) << 40);
+  h->level = st;
   __threadfence();
   atomicExch(&h->claim, (static_cast<unsigned long long>(gen) << 32) |
-                            (static_cast<unsigned long long>(w) << 27));
+                            (static_cast<unsigned long long>(st) << 26));
   __threadfence();
-  srv_push_job(a, gen, w, slot);
+  srv_push_job(a, gen, st, slot);
   atomicAdd(&a.dh->levels_opened, 1ull);
 }
 
-// After levels 1..w of a request: settle it (a witness below the target,
-// the bound met, or every level done) or open level w + 1.  One thread.
+// After stage st of a request: settle it (a witness below the target, the
+// bound met, or every level done) or open stage st + 1.  After part 1 of
+// level w the unseen codewords weigh at least ceil(49 w / (k - 1)); after
+// part 2, ceil(49 (w + 1) / k).  Part 2 of level k has no support.  One
+// thread.
 __device__ void srv_level_end(const SrvArgs& a, unsigned int slot, SrvSlotHdr* h,
-                              unsigned int gen, int w) {
+                              unsigned int gen, int st) {
   __threadfence();
   const int best = atomicAdd(&h->best, 0);
   const int k = __ldcg(&h->k);
@@ -176,12 +196,14 @@ __device__ void srv_level_end(const SrvArgs& a, unsigned int slot, SrvSlotHdr* h
     srv_settle(a, slot, h, kN - best, true);
     return;
   }
-  const int bound = (kN * (w + 1) + k - 1) / k;
+  const int w = srv_stage_level(st);
+  const int bound = srv_stage_part(st) == 1 ? (kN * w + k - 2) / (k - 1)  // k >= w >= 4
+                                            : (kN * (w + 1) + k - 1) / k;
   if (w >= k || best <= bound) {
     srv_settle(a, slot, h, kN - best, false);
     return;
   }
-  srv_open_level(a, slot, h, gen, w + 1);
+  srv_open_level(a, slot, h, gen, st + 1);
 }
 
 // Evaluates a request whose indices are in h->idx (warp-level): one
@@ -232,7 +254,7 @@ __device__ void srv_evaluate(const SrvArgs& a, int lane, unsigned int slot, SrvS
     } else {
       __threadfence();
       *reinterpret_cast<volatile unsigned int*>(&h->state) = kSlotRun;
-      srv_open_level(a, slot, h, gen, 4);
+      srv_open_level(a, slot, h, gen, kSrvFirstStage);
     }
   }
   __syncwarp();
@@ -365,21 +387,24 @@ __device__ void srv_resolve(const SrvArgs& a, int lane, unsigned int slot, uint8
 }
 
 // Runs the 32 tasks a warp claimed: `cw` is the claim word's value before
-// the warp's atomicAdd (request gen, level w, first task t0).  A claim on a
-// slot that no longer serves gen, or past the level's end, runs nothing.
-// The warp that counts a level's last task ends the level.
+// the warp's atomicAdd (request gen, stage st, first task t0).  A claim on a
+// slot that no longer serves gen, or past the stage's end, runs nothing.
+// The warp that counts a stage's last task ends the stage.
 __device__ void srv_run(const SrvArgs& a, int lane, unsigned int slot, unsigned long long cw,
                         const unsigned long long (*bn)[kIsBinom], uint16_t* dig, uint32_t* ez,
                         unsigned long long& n_tasks, unsigned long long& n_codewords) {
   SrvSlotHdr* h = srv_slot(a, slot);
   const unsigned int gen = static_cast<unsigned int>(cw >> 32);
-  const int w = static_cast<int>((cw >> 27) & 31ull);
+  const int st = static_cast<int>((cw >> 26) & 63ull);
+  const int w = srv_stage_level(st);
   const unsigned long long t0 = cw & kSrvTaskMask;
-  if (ld_vol32(&h->id) != gen || w < 4) return;
+  if (ld_vol32(&h->id) != gen || st < kSrvFirstStage) return;
   __threadfence();
   const int k = __ldcg(&h->k);
   const int tmax = __ldcg(&h->tmax);
-  const unsigned long long units = srv_units(bn, k, w);
+  unsigned long long n_sup, s_off;
+  srv_supports(bn, k, st, n_sup, s_off);
+  const unsigned long long units = n_sup * is_units_per_support(w);
   const unsigned long long nb = srv_task_units(units, w, a.lanes);
   const unsigned long long nt = (units + nb - 1ull) / nb;
   if (t0 >= nt) return;
@@ -392,7 +417,8 @@ __device__ void srv_run(const SrvArgs& a, int lane, unsigned int slot, unsigned 
     const unsigned long long u1 = min(u0 + nb, units);
     wmin = is_walk_range<kSrvTPB, false, true>(srv_rows(a, h), 1, 0, &h->abort,
                                                WitSrc{nullptr, nullptr, nullptr}, bn, dig, ez,
-                                               k, w, u0, u1, wthr, ld_flag(&h->best), ncw);
+                                               k, w, n_sup, s_off, u0, u1, wthr,
+                                               ld_flag(&h->best), ncw);
   }
   const int wl = __reduce_min_sync(0xffffffffu, wmin);
   for (int o = 16; o > 0; o >>= 1) ncw += __shfl_xor_sync(0xffffffffu, ncw, o);
@@ -415,8 +441,8 @@ __device__ void srv_run(const SrvArgs& a, int lane, unsigned int slot, unsigned 
     const unsigned long long add = owned + skipped;
     const unsigned long long old = atomicAdd(&h->done, add);
     n_tasks += owned;
-    if ((old >> 40) == static_cast<unsigned long long>(w) && (old & kSrvDoneMask) + add == nt)
-      srv_level_end(a, slot, h, gen, w);
+    if ((old >> 40) == static_cast<unsigned long long>(st) && (old & kSrvDoneMask) + add == nt)
+      srv_level_end(a, slot, h, gen, st);
   }
   __syncwarp();
 }
@@ -489,10 +515,10 @@ __global__ void __launch_bounds__(kSrvTPB, kSrvPerSm) serve_kernel(SrvArgs a) {
           const unsigned long long e = ld_vol64(je);
           if (e == 0ull) break;  // pushed but not yet written
           const unsigned int gen = static_cast<unsigned int>(e >> 32);
-          const int w = static_cast<int>((e >> 24) & 0xFFull);
+          const int st = static_cast<int>((e >> 24) & 0xFFull);
           const unsigned int sl = static_cast<unsigned int>(e & 0xFFFFFFull);
           SrvSlotHdr* h = srv_slot(a, sl);
-          if (w == 0) {
+          if (st == 0) {
             // a waiting request: take the job; resolve it once its
             // equivalent's answer is final, else put it back behind the rest
             if (atomicCAS(&a.dh->job_head.v, hd, hd + 1u) != hd) continue;
@@ -510,12 +536,13 @@ __global__ void __launch_bounds__(kSrvTPB, kSrvPerSm) serve_kernel(SrvArgs a) {
             continue;
           }
           const unsigned long long tag = (static_cast<unsigned long long>(gen) << 32) |
-                                         (static_cast<unsigned long long>(w) << 27);
+                                         (static_cast<unsigned long long>(st) << 26);
           const unsigned long long cur = ld_vol64(&h->claim);
           bool open = false;
           if ((cur & ~kSrvTaskMask) == tag) {
             const int k = __ldcg(&h->k);
-            const unsigned long long units = srv_units(s_binom, k, w);
+            const int w = srv_stage_level(st);
+            const unsigned long long units = srv_units(s_binom, k, st);
             const unsigned long long nt =
                 (units + srv_task_units(units, w, a.lanes) - 1ull) /
                 srv_task_units(units, w, a.lanes);

@@ -65,9 +65,10 @@ static int srv_defaults(const tg_server_params* p, tg_server_params& q) {
 
 // Job ring capacity: a power of two above every job a full pool of requests
 // can have pushed and not yet popped (each request pushes at most one job
-// per level, k - 3 <= 18 levels, plus wait jobs that replace one another).
+// per stage, two per level for k - 3 <= 18 levels, plus wait jobs that
+// replace one another).
 static unsigned int srv_job_capacity(int S) {
-  unsigned long long need = 32ull * static_cast<unsigned long long>(S) + 1024ull;
+  unsigned long long need = 40ull * static_cast<unsigned long long>(S) + 1024ull;
   unsigned long long J = 1024ull;
   while (J < need) J <<= 1;
   return static_cast<unsigned int>(J);

@@ -25,6 +25,7 @@ from __future__ import annotations
 
 import itertools
 import random
+from math import comb
 
 import pytest
 
@@ -153,3 +154,43 @@ def test_levels123_unranking_covers_every_support(k):
     got = unrank_small_levels(k)
     want = [c for w in (1, 2, 3) for c in itertools.combinations(range(k), w)]
     assert sorted(got) == sorted(want) and len(got) == len(want)
+
+
+def unrank_support(k: int, w: int, rank: int) -> tuple[int, ...]:
+    """Rows of the support of rank `rank` at level w, unranked as
+    is_walk_range does: from row k - 1 down, take row pos when the remaining
+    rank is at least C(pos, rem)."""
+    rows, rem = [], w
+    for pos in range(k - 1, -1, -1):
+        if rem == 0:
+            break
+        b = comb(pos, rem)
+        if rank < b:
+            continue
+        rank -= b
+        rem -= 1
+        rows.append(pos)
+    assert rem == 0
+    return tuple(sorted(rows))
+
+
+def part_supports(k: int, w: int, part: int) -> tuple[int, int]:
+    """(count, first rank) of a toric code's supports in part `part` of level
+    w, as is_part_supports gives them."""
+    if part == 1:
+        return comb(k - 1, w - 1), comb(k - 1, w)
+    return comb(k - 1, w), 0
+
+
+@pytest.mark.parametrize("k", [4, 5, 9, 14])
+def test_level_parts_split_supports_by_the_last_row(k):
+    """Part 1 of level w holds exactly the supports with row k - 1, part 2
+    the others; together every w-subset of the rows once."""
+    for w in range(4, k + 1):
+        seen = []
+        for part in (1, 2):
+            n_sup, s_off = part_supports(k, w, part)
+            sup = [unrank_support(k, w, s_off + s) for s in range(n_sup)]
+            assert all(((k - 1) in x) == (part == 1) for x in sup)
+            seen += sup
+        assert sorted(seen) == list(itertools.combinations(range(k), w))
