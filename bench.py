@@ -850,6 +850,7 @@ def run_b200_arm(args, d: Dist) -> None:
     check = d_out.cpu().tolist()
     tasks, codewords, ref_msgs = runner.counters(stream)
     paths = runner.path_counters(stream)
+    stages = runner.stage_counters(stream)
 
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
     clocks = clock_sampler(dev)
@@ -985,6 +986,7 @@ def run_b200_arm(args, d: Dist) -> None:
             "codes_per_s": d.world * len(sets) / (total_ms / 1e3 / args.steps),
             "evaluated_codewords_per_s": d.world * codewords / (total_ms / 1e3 / args.steps),
             "evaluated_codewords_per_step": codewords, "path_counters": paths,
+            "infoset_codewords_by_stage": stages,
             "prep_ms": statistics.mean(prep_ms), "enumeration_walk_ms": statistics.mean(enum_ms),
             "infoset_walk_ms": statistics.mean(is_ms),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),

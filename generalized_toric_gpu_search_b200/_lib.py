@@ -80,6 +80,10 @@ SIGNATURES: dict[str, tuple] = {
         [c_void_p, c_void_p, c_void_p, POINTER(c_uint64), POINTER(c_uint64), POINTER(c_double)],
     ),
     "tg_distance_path_counters": (c_int, [c_void_p, c_void_p, c_void_p, POINTER(c_uint64)]),
+    "tg_distance_stage_counters": (
+        c_int,
+        [c_void_p, c_void_p, c_void_p, POINTER(c_uint64), c_int32],
+    ),
     "tg_canonical_sets": (
         c_int,
         [c_void_p, c_void_p, c_int32, c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p],

@@ -539,6 +539,31 @@ int tg_distance_path_counters(const tg_distance_params* p, const void* d_workspa
   return TG_OK;
 }
 
+static_assert(kIsStages == TG_INFOSET_STAGES, "stage count of the header");
+
+int tg_distance_stage_counters(const tg_distance_params* p, const void* d_workspace, void* stream,
+                               uint64_t* h_counts, int32_t n) {
+  int st = check_distance_params(p);
+  if (st) return st;
+  if (!d_workspace || !h_counts) return invalid("tg_distance_stage_counters: NULL argument");
+  if (n < 0) return invalid("tg_distance_stage_counters: n must be >= 0");
+  const WsLayout L = ws_layout(*p);
+  IsHeader hi{};
+  if (L.is_min_k <= p->k_max && p->n_sets > 0) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemcpyAsync(&hi, static_cast<const uint8_t*>(d_workspace) + L.is_hdr,
+                                    sizeof(hi), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(e, "tg_distance_stage_counters");
+  }
+  // Levels 1 to 3 add to the total only (one warp per set; no second atomic).
+  unsigned long long later = 0ull;
+  for (int i = 1; i < kIsStages; ++i) later += hi.stage_codewords[i];
+  hi.stage_codewords[0] = hi.codewords - later;
+  for (int i = 0; i < n && i < kIsStages; ++i) h_counts[i] = hi.stage_codewords[i];
+  return TG_OK;
+}
+
 int tg_canonical_sets(tg_context* ctx, const int32_t* d_sets, int32_t n, int32_t k,
                       uint64_t* d_out_mask, uint64_t* d_out_key_lo, uint64_t* d_out_key_hi,
                       int32_t* d_status, void* stream) {

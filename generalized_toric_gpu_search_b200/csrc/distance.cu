@@ -928,7 +928,7 @@ int run_walk(const DistArgs& args, int sm_count, int blocks_per_sm, int tpb, cud
     const int per_sm = args.is_blocks_per_sm > 0 ? min(args.is_blocks_per_sm, kPerSm) : kPerSm;
     la.is_lanes = sm_count * per_sm * kIsWalkThreads;
     const int plan_grid = (args.n + 255) / 256;
-    levels123_kernel<<<(args.n + 3) / 4, 128, 0, s>>>(la);
+    levels123_kernel<<<args.n, kL123Threads, 0, s>>>(la);
     const int w_last = infoset_last_level(args.k_max, args.is_toric);
     // Each level in two parts (a toric code's supports with and without its
     // last row; other codes walk the whole level in part 1).

@@ -16,6 +16,10 @@ struct WsHeader {
 };
 
 // Header of the information-set walk (one level at a time).
+// Stages of the information-set walk: 0 = levels 1 to 3 (one launch), then
+// 2 w + part - 1 for part 1 or 2 of level w >= 4.
+constexpr int kIsStages = 2 * kMaxExactK + 2;
+
 struct IsHeader {
   unsigned long long counter;    // next unclaimed task of the level being walked
   unsigned long long total;      // tasks of that level
@@ -24,6 +28,7 @@ struct IsHeader {
   unsigned long long codewords;  // codewords evaluated
   int32_t level;
   int32_t work;                  // set by plan_level_kernel when some set needs the level
+  unsigned long long stage_codewords[kIsStages];  // codewords evaluated per stage
 };
 
 // Per-code descriptor written by the prep kernels.

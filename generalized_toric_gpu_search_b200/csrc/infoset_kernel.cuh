@@ -990,33 +990,37 @@ __device__ __forceinline__ int is_walk_range(const V6* base, int n_sets, int del
     // row found is Gray digit q (q < w - 1); the last one has coefficient 1.
     // Digit 0 is swept through all seven values and stays out of P; digit 1
     // starts every block at alpha^0; digit 2 + i starts at the Gray value of
-    // base-7 digit i of b.
-    V6 P;
-    v6_zero(P);
-    uint32_t r0 = 0u, r1 = 0u;
-    unsigned long long srank = s + s_off, rest = b;
-    int rem = w, q = 0;
-    for (int pos = k - 1; pos >= 0 && rem > 0; --pos) {
-      const unsigned long long bb = bn[pos][rem];
-      if (srank < bb) continue;
-      srank -= bb;
-      --rem;
-      const uint32_t R = uint32_t(pos * kIsVecPerRow);
-      if (rem > 0 && q == 0) {
-        r0 = R;
-      } else {
-        V6 g = v6_load<kCG>(rows + R);
-        if (rem > 0) {
-          if (q == 1) {
-            r1 = R;
-          } else {
-            dig[(q - 2) * kStride] = uint16_t(R);
-            v6_alpha_pow(g, is_block_digit(rest));
-          }
+    // base-7 digit i of b.  The positions are found first, by a loop whose
+    // body is a few predicated instructions (every lane runs all k steps, so
+    // the warp stays converged whatever its lanes' supports), and the rows
+    // are loaded after it, by a loop over the w digits.
+    uint32_t r0 = 0u, r1 = 0u, rl = 0u;
+    {
+      unsigned long long srank = s + s_off;
+      int rem = w, q = 0;
+      for (int pos = k - 1; pos >= 0; --pos) {
+        const unsigned long long bb = bn[pos][rem];
+        if (rem > 0 && srank >= bb) {
+          const uint32_t R = uint32_t(pos * kIsVecPerRow);
+          if (rem == 1) rl = R;
+          else if (q == 0) r0 = R;
+          else if (q == 1) r1 = R;
+          else dig[(q - 2) * kStride] = uint16_t(R);
+          srank -= bb;
+          --rem;
+          ++q;
         }
+      }
+    }
+    V6 P = v6_load<kCG>(rows + rl);
+    if (w >= 3) v6_xor(P, v6_load<kCG>(rows + r1));
+    {
+      unsigned long long rest = b;
+      for (int i = 0; i < w - 3; ++i) {
+        V6 g = v6_load<kCG>(rows + dig[i * kStride]);
+        v6_alpha_pow(g, is_block_digit(rest));
         v6_xor(P, g);
       }
-      ++q;
     }
     if (w == 1) {
       const int wt = __popc(lop3<0xFE>(P.l0, P.l1, P.l2)) + __popc(lop3<0xFE>(P.h0, P.h1, P.h2));
@@ -1141,25 +1145,29 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) walk_level_kernel(DistArgs a
     }
   }
   for (int o = 16; o > 0; o >>= 1) evaluated += __shfl_xor_sync(0xffffffffu, evaluated, o);
-  if (lane == 0 && evaluated) atomicAdd(&a.is_hdr->codewords, evaluated);
+  if (lane == 0 && evaluated) {
+    atomicAdd(&a.is_hdr->codewords, evaluated);
+    atomicAdd(&a.is_hdr->stage_codewords[2 * w + part - 1], evaluated);
+  }
 }
 
-// Levels 1 to 3 of n_sets information sets of k rows (at base), by one warp:
-// the rows themselves (weight-1 messages); for each pair of rows q < p the
-// sweep alpha^v row_p + row_q; for each triple q < p < t the seven sweeps
-// alpha^v row_t + alpha^s row_p + row_q (messages up to scalars).  Returns
-// the smallest weight, reduced over the warp; ncw = codewords evaluated.
-// With wsrc.dst set (the witness pass) the first codeword lighter than wthr
-// is recorded.  kCG: the rows may have been written during the launch.
+// Levels 1 to 3 of n_sets information sets of k rows (at base), by nthr
+// threads (this one is tid): the rows themselves (weight-1 messages); for
+// each pair of rows q < p the sweep alpha^v row_p + row_q; for each triple
+// q < p < t the seven sweeps alpha^v row_t + alpha^s row_p + row_q
+// (messages up to scalars).  Returns this thread's smallest weight; ncw =
+// codewords evaluated by all nthr threads.  With wsrc.dst set (the witness
+// pass) the first codeword lighter than wthr is recorded.  kCG: the rows may
+// have been written during the launch.
 template <bool kCG>
-__device__ int is_levels123_sets(int lane, const V6* base, int n_sets, int k, WitSrc wsrc,
-                                 int wthr, unsigned long long& ncw) {
+__device__ int is_levels123_part(int tid, int nthr, const V6* base, int n_sets, int k,
+                                 WitSrc wsrc, int wthr, unsigned long long& ncw) {
   const int n1 = k, n2 = k * (k - 1) / 2, n3 = k * (k - 1) * (k - 2) / 6;
   const int per_set = n1 + n2 + n3;
   const int total = n_sets * per_set;
   const bool wit = wsrc.dst != nullptr;
   int wmin = kN + 1;
-  for (int u = lane; u < total; u += 32) {
+  for (int u = tid; u < total; u += nthr) {
     const int j = u / per_set;
     int r = u - j * per_set;
     const V6* rows = base + size_t(j) * k * kIsVecPerRow;
@@ -1197,32 +1205,48 @@ __device__ int is_levels123_sets(int lane, const V6* base, int n_sets, int k, Wi
       }
     }
   }
-  for (int o = 16; o > 0; o >>= 1) wmin = min(wmin, __shfl_xor_sync(0xffffffffu, wmin, o));
   ncw = static_cast<unsigned long long>(n_sets) *
         static_cast<unsigned long long>(n1 + 7 * n2 + 49 * n3);
   return wmin;
 }
 
-// Levels 1 to 3 of every set of a batch in one launch, one warp per set.
-// These levels are too small to fill the GPU one launch each, and running
-// them without the bound check between them only adds codewords (the best
-// weight stays that of a codeword); level 4 onwards then follows the plan /
-// scan / walk triple.
-__global__ void __launch_bounds__(128) levels123_kernel(DistArgs a) {
-  const int lane = threadIdx.x & 31;
-  const int c = blockIdx.x * 4 + (threadIdx.x >> 5);
-  if (c >= a.n) return;  // warp-uniform
+// is_levels123_part by one warp, the smallest weight reduced over it.
+template <bool kCG>
+__device__ int is_levels123_sets(int lane, const V6* base, int n_sets, int k, WitSrc wsrc,
+                                 int wthr, unsigned long long& ncw) {
+  int wmin = is_levels123_part<kCG>(lane, 32, base, n_sets, k, wsrc, wthr, ncw);
+  for (int o = 16; o > 0; o >>= 1) wmin = min(wmin, __shfl_xor_sync(0xffffffffu, wmin, o));
+  return wmin;
+}
+
+// Levels 1 to 3 of every set of a batch in one launch, one CTA of
+// kL123Threads per set (a 14-row set has 469 row, pair and triple units, so
+// the larger sets no longer hold one warp each for the whole launch).  These
+// levels are too small to fill the GPU one launch each, and running them
+// without the bound check between them only adds codewords (the best weight
+// stays that of a codeword); level 4 onwards then follows the plan / scan /
+// walk triples.
+constexpr int kL123Threads = 128;
+
+__global__ void __launch_bounds__(kL123Threads) levels123_kernel(DistArgs a) {
+  __shared__ int s_min[kL123Threads / 32];
+  const int c = blockIdx.x;
+  const int tid = threadIdx.x;
   const CodeDesc d = a.desc[c];
   if ((d.flags & kIsCodeFlag) == 0 || (d.flags & kDecidedFlag) != 0 || ld_flag(a.abort + c) != 0)
-    return;
+    return;  // uniform over the CTA
   // The witness pass records the first codeword lighter than the target.
   const WitSrc wsrc = a.witness ? WitSrc{a.is_piv + size_t(c) * kIsMaxSets,
                                          a.witness + size_t(c) * kN, a.wit_lock + c}
                                 : WitSrc{nullptr, nullptr, nullptr};
   unsigned long long ncw = 0ull;
-  const int wmin = is_levels123_sets<false>(lane, a.is_rows + size_t(c) * a.is_stride, d.H, d.k,
-                                            wsrc, kN - d.tmax, ncw);
-  if (lane == 0) {
+  int wmin = is_levels123_part<false>(tid, kL123Threads, a.is_rows + size_t(c) * a.is_stride, d.H,
+                                      d.k, wsrc, kN - d.tmax, ncw);
+  for (int o = 16; o > 0; o >>= 1) wmin = min(wmin, __shfl_xor_sync(0xffffffffu, wmin, o));
+  if ((tid & 31) == 0) s_min[tid >> 5] = wmin;
+  __syncthreads();
+  if (tid == 0) {
+    for (int i = 1; i < kL123Threads / 32; ++i) wmin = min(wmin, s_min[i]);
     atomicAdd(&a.is_hdr->codewords, ncw);
     if (wmin < a.is_best[c]) a.is_best[c] = wmin;
     if (a.is_best[c] < kN - d.tmax) a.abort[c] = 1;  // a witness below the target distance

@@ -322,6 +322,23 @@ class DistanceRunner:
         return {"enumeration_tasks": int(h[0]), "enumeration_codewords": int(h[1]),
                 "infoset_tasks_queued": int(h[2]), "infoset_codewords": int(h[3])}
 
+    def stage_counters(self, stream: torch.cuda.Stream | None = None) -> dict[str, int]:
+        """Codewords of the last run's information-set walk per stage: "1-3"
+        (levels 1 to 3), then "w.1" and "w.2" for the two parts of level w
+        (stages with no codeword are left out)."""
+        st = stream if stream is not None else torch.cuda.current_stream(self.device)
+        n = 2 * 21 + 2
+        h = (ctypes.c_uint64 * n)()
+        _lib.check(_lib.load().tg_distance_stage_counters(ctypes.byref(self.last_params),
+                                                          self._ws.data_ptr(), st.cuda_stream,
+                                                          h, n),
+                   "tg_distance_stage_counters")
+        out = {"1-3": int(h[0])} if h[0] else {}
+        for i in range(1, n):
+            if h[i]:
+                out["%d.%d" % (i // 2, 2 if i % 2 else 1)] = int(h[i])
+        return out
+
 
 class DistanceOracleCUDABP:
     """Drop-in for the reference's DistanceOracleCUDABP (kernel_cuda_bp.py:246-323).

@@ -251,6 +251,16 @@ int tg_distance_counters(const tg_distance_params* p, const void* d_workspace,
 int tg_distance_path_counters(const tg_distance_params* p, const void* d_workspace,
                               void* stream, uint64_t* h_counts);
 
+/* Codewords the information-set walk evaluated per stage (synchronises
+ * `stream`): h_counts[0] = levels 1 to 3, h_counts[2 w + part - 1] = part
+ * `part` (1 or 2) of level w >= 4.  Part 1 of a level takes the supports
+ * holding the set's last row, part 2 the others (a non-toric matrix walks
+ * whole levels in part 1).  Writes min(n, TG_INFOSET_STAGES) entries.  No
+ * counterpart in the reference (profiling aid). */
+#define TG_INFOSET_STAGES 44
+int tg_distance_stage_counters(const tg_distance_params* p, const void* d_workspace,
+                               void* stream, uint64_t* h_counts, int32_t n);
+
 /* ---- canonical forms ---------------------------------------------------- */
 
 /* Canonical form of n exponent sets given as rows of a (n, k) int32 matrix.

@@ -194,3 +194,4 @@ def test_level_parts_split_supports_by_the_last_row(k):
             assert all(((k - 1) in x) == (part == 1) for x in sup)
             seen += sup
         assert sorted(seen) == list(itertools.combinations(range(k), w))
+
