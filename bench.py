@@ -82,11 +82,11 @@ def last_infoset_level(k_max: int) -> int:
 
 def launches_per_step(k_max: int, enumeration: str) -> int:
     """Kernels per step: prep_exact, scan_tasks and the enumeration walk; with
-    information sets also prep_infoset, levels123 (levels 1 to 3), per level
-    4..last_infoset_level(k_max) two parts of plan, scan and walk each, and
-    finalize_infoset."""
+    information sets also prep_infoset, order_codes, levels123 (levels 1 to
+    3), per level 4..last_infoset_level(k_max) two parts of plan, scan and
+    walk each, and finalize_infoset."""
     infoset = enumeration == "infoset" or (enumeration == "auto" and k_max >= 2)
-    return 3 + ((3 + 6 * max(0, last_infoset_level(k_max) - 3)) if infoset else 0)
+    return 3 + ((4 + 6 * max(0, last_infoset_level(k_max) - 3)) if infoset else 0)
 
 
 L2_FLUSH_BYTES = 256 << 20

@@ -259,6 +259,7 @@ static void bind_workspace(DistArgs& a, const WsLayout& L, void* ws) {
   a.is_units = reinterpret_cast<uint64_t*>(b + L.is_units);
   a.is_off = reinterpret_cast<uint64_t*>(b + L.is_off);
   a.is_best = reinterpret_cast<int32_t*>(b + L.is_best);
+  a.is_perm = reinterpret_cast<int32_t*>(b + L.is_perm);
 }
 
 // Validates a max_zeros call and fills the kernel arguments.

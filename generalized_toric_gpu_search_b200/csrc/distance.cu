@@ -141,6 +141,7 @@ WsLayout ws_layout(const tg_distance_params& p) {
   L.is_units = off; off = align256(off + n_is * sizeof(uint64_t));
   L.is_off = off;   off = align256(off + (infoset ? n + 1 : 0) * sizeof(uint64_t));
   L.is_best = off;  off = align256(off + n_is * sizeof(int32_t));
+  L.is_perm = off;  off = align256(off + n_is * sizeof(int32_t));
   L.total = off;
   return L;
 }
@@ -895,6 +896,7 @@ int run_prepare(const DistArgs& args, cudaStream_t s) {
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(information-set header)");
     prep_infoset_kernel<<<(args.n + kIsPrepWarps - 1) / kIsPrepWarps, kIsPrepWarps * 32, 0, s>>>(
         args);
+    order_codes_kernel<<<1, kScanThreads, 0, s>>>(args);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "information-set prep launch");
   }

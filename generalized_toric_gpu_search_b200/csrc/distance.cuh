@@ -67,7 +67,7 @@ __host__ __device__ constexpr int infoset_max_sets(int k) {
 
 struct WsLayout {
   size_t hdr, desc, task_off, abort, basis, pat_cum, pat_info, bitpat;
-  size_t is_hdr, is_rows, is_units, is_off, is_best, total;
+  size_t is_hdr, is_rows, is_units, is_off, is_best, is_perm, total;
   int basis_stride, pat_stride, bitpat_stride, is_stride, is_min_k;
 };
 
@@ -107,7 +107,8 @@ struct DistArgs {
   IsHeader* is_hdr;              // task queue of the information-set walk
   V6* is_rows;                   // per code and set: k rows x (g, 6 deltas)
   uint64_t* is_units;            // units of the current level per code
-  uint64_t* is_off;              // task offsets of the current level (n + 1)
+  uint64_t* is_off;              // task offsets of the current level per code position (n + 1)
+  int32_t* is_perm;              // code at each position (codes ordered by k)
   int32_t* is_best;              // smallest weight met per code
   // Witness pass only (NULL otherwise): per code and set the pivot columns
   // (kIsMaxSets words), the witness codewords (49 GF(8) symbols per code, in

@@ -316,6 +316,32 @@ __device__ __forceinline__ unsigned long long is_max_task_units(int w) {
   return w >= 3 ? 343ull : (w == 2 ? 2401ull : 16807ull);
 }
 
+// Orders the codes by k for the level walks (is_perm: position -> code).
+// Tasks are numbered over positions, so where a warp's 32 tasks span two
+// codes those have the same k, the same loop lengths and, mostly, the same
+// threshold mode (in batch order, with k mixed, C2 ran 3 % slower).  One CTA;
+// the order within a k is that of the atomics (it changes no result).
+__global__ void __launch_bounds__(kScanThreads) order_codes_kernel(DistArgs a) {
+  __shared__ int s_cnt[kIsBinom + 1];
+  const int t = threadIdx.x;
+  for (int i = t; i <= kIsBinom; i += kScanThreads) s_cnt[i] = 0;
+  __syncthreads();
+  for (int c = t; c < a.n; c += kScanThreads)
+    atomicAdd(&s_cnt[max(0, min(a.desc[c].k, kIsBinom))], 1);
+  __syncthreads();
+  if (t == 0) {
+    int run = 0;
+    for (int i = 0; i <= kIsBinom; ++i) {
+      const int x = s_cnt[i];
+      s_cnt[i] = run;
+      run += x;
+    }
+  }
+  __syncthreads();
+  for (int c = t; c < a.n; c += kScanThreads)
+    a.is_perm[atomicAdd(&s_cnt[max(0, min(a.desc[c].k, kIsBinom))], 1)] = c;
+}
+
 // Level w of a toric code runs in two parts.  Part 1 takes the supports that
 // hold the last row (index k - 1): C(k-1, w-1) of them, support ranks
 // C(k-1, w) .. C(k, w) - 1.  Part 2 takes the others: C(k-1, w), ranks
@@ -386,7 +412,8 @@ __global__ void plan_level_kernel(DistArgs a, int w, int part) {
 }
 
 // Task size of level w (units per task, sized so the level has about eight
-// tasks per resident thread) and the per-code task offsets.  One CTA.
+// tasks per resident thread) and the task offsets of the code positions (the
+// codes in is_perm order).  One CTA.
 __global__ void __launch_bounds__(kScanThreads) scan_level_kernel(DistArgs a, int w) {
   __shared__ unsigned long long s_part[kScanThreads / 32];
   __shared__ unsigned long long s_nb;
@@ -412,7 +439,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_level_kernel(DistArgs a, in
   unsigned long long sum = 0ull;
   bool over = false;
   for (int i = beg; i < end; ++i) {
-    const unsigned long long x = a.is_units[i];
+    const unsigned long long x = a.is_units[a.is_perm[i]];
     if (sum + x < sum) over = true;
     sum += x;
   }
@@ -456,7 +483,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_level_kernel(DistArgs a, in
   const unsigned long long nb = s_nb;
   // pass 2: tasks per code, exclusive scan
   unsigned long long tsum = 0ull;
-  for (int i = beg; i < end; ++i) tsum += (a.is_units[i] + nb - 1ull) / nb;
+  for (int i = beg; i < end; ++i) tsum += (a.is_units[a.is_perm[i]] + nb - 1ull) / nb;
   unsigned long long incl = tsum;
   for (int o = 1; o < 32; o <<= 1) {
     const unsigned long long y = __shfl_up_sync(0xffffffffu, incl, o);
@@ -477,7 +504,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_level_kernel(DistArgs a, in
   unsigned long long run = incl - tsum + (wid > 0 ? s_part[wid - 1] : 0ull);
   for (int i = beg; i < end; ++i) {
     a.is_off[i] = run;
-    run += (a.is_units[i] + nb - 1ull) / nb;
+    run += (a.is_units[a.is_perm[i]] + nb - 1ull) / nb;
   }
   __syncthreads();
   if (t == 0) {
@@ -818,9 +845,11 @@ __device__ __forceinline__ int is_block_fix(unsigned fl, Pl3 W, Pl3 Pz, const ui
 
 // Smallest thr at which a block is tested on pairs of codewords (with seven
 // selections of about 7/64 of the 32 low columns each, a pair's count tops 15
-// in about 0.3 % of the sweeps, against 1.3e-5 for the largest single count
-// over 14).
-constexpr int kIsPairThr = 15;
+// in about 0.3 % of the sweeps and 16 in about 0.08 %, against 1.3e-5 for the
+// largest single count over 14).  At thr = 15 about half of a warp's blocks
+// hold a flagged sweep, and counting it leaves the other lanes idle: single
+// counts there made C2 0.9 % faster.
+constexpr int kIsPairThr = 16;
 
 // Walks blocks [b0, b0 + nblk) of one support; P is the sum of its rows other
 // than digit 0 at the start of block b0.  Each block is 7 sweeps of digit 0
@@ -1085,16 +1114,19 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) walk_level_kernel(DistArgs a
   unsigned long long evaluated = 0ull;
   uint16_t* my_dig = &s_dig[0][threadIdx.x];  // this thread's digit rows, stride kTPB
   uint32_t* my_ez = &s_ez[0][threadIdx.x];     // this thread's digit-1 moves, stride kTPB
-  int c0 = 0;  // code of the warp's first task; tasks are claimed in increasing order
+  // Tasks are numbered over code positions (codes ordered by k, is_perm);
+  // p0 is the position of the warp's first task, claimed in increasing order.
+  int p0 = 0;
   for (;;) {
     unsigned long long base = 0ull;
     if (lane == 0) base = atomicAdd(&a.is_hdr->counter, 32ull);
     base = __shfl_sync(0xffffffffu, base, 0);
     if (base >= total) break;
-    if (lane == 0) c0 = last_le_from(a.is_off, c0, a.n + 1, base);
-    c0 = __shfl_sync(0xffffffffu, c0, 0);
+    if (lane == 0) p0 = last_le_from(a.is_off, p0, a.n + 1, base);
+    p0 = __shfl_sync(0xffffffffu, p0, 0);
     // The code's abort flag and best weight sit in a few cache lines that
     // every lane would poll, so lane 0 reads them for the warp's first code.
+    const int c0 = __ldg(a.is_perm + p0);
     int abort0 = 0, best0 = 0;
     if (lane == 0) {
       abort0 = ld_flag(a.abort + c0);
@@ -1103,18 +1135,19 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) walk_level_kernel(DistArgs a
     abort0 = __shfl_sync(0xffffffffu, abort0, 0);
     best0 = __shfl_sync(0xffffffffu, best0, 0);
     const unsigned long long t = base + lane;
-    int c = -1, wmin = kN + 1;
+    int c = -1, p = -1, wmin = kN + 1;
     if (t < total) {
-      c = t < __ldg(a.is_off + c0 + 1) ? c0 : last_le_from(a.is_off, c0, a.n + 1, t);
-      if (c != c0) {
+      p = t < __ldg(a.is_off + p0 + 1) ? p0 : last_le_from(a.is_off, p0, a.n + 1, t);
+      c = p == p0 ? c0 : __ldg(a.is_perm + p);
+      if (p != p0) {
         abort0 = ld_flag(a.abort + c);
         best0 = ld_flag(a.is_best + c);
       }
       if (abort0) {
-        atomicMax(&a.is_hdr->counter, __ldg(a.is_off + c + 1));
+        atomicMax(&a.is_hdr->counter, __ldg(a.is_off + p + 1));
         c = -1;
       } else {
-        const unsigned long long u0 = (t - __ldg(a.is_off + c)) * nb;
+        const unsigned long long u0 = (t - __ldg(a.is_off + p)) * nb;
         const unsigned long long u1 =
             min(u0 + nb, static_cast<unsigned long long>(a.is_units[c]));
         unsigned long long ncw = 0ull;
@@ -1131,6 +1164,7 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) walk_level_kernel(DistArgs a
     for (unsigned pend = __ballot_sync(0xffffffffu, c >= 0); pend != 0u;) {
       const int leader = __ffs(pend) - 1;
       const int cl = __shfl_sync(0xffffffffu, c, leader);
+      const int pl = __shfl_sync(0xffffffffu, p, leader);
       const bool mine = c == cl;
       const int wl = __reduce_min_sync(0xffffffffu, mine ? wmin : kN + 1);
       pend &= ~__ballot_sync(0xffffffffu, mine);
@@ -1139,7 +1173,7 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) walk_level_kernel(DistArgs a
         if (best < kN - a.desc[cl].tmax) {
           // a witness below the target distance: the code is decided
           atomicExch(a.abort + cl, 1);
-          atomicMax(&a.is_hdr->counter, __ldg(a.is_off + cl + 1));
+          atomicMax(&a.is_hdr->counter, __ldg(a.is_off + pl + 1));
         }
       }
     }

@@ -78,11 +78,12 @@ def test_max_over_ranks_gloo_world2():
 
 def test_launches_per_step_follow_the_level_structure():
     """gpu_launches counts: prep_exact, scan_tasks and the enumeration walk;
-    with information sets also prep_infoset, levels123 (levels 1-3), two
-    plan / scan / walk triples (the two parts) per level 4..the last level the
-    Griesmer cap leaves (9 for k_max = 14, 11 for 21), and finalize_infoset."""
-    assert bench.launches_per_step(14, "auto") == 3 + 3 + 6 * 6
-    assert bench.launches_per_step(3, "auto") == 3 + 3
+    with information sets also prep_infoset, order_codes, levels123 (levels
+    1-3), two plan / scan / walk triples (the two parts) per level 4..the last
+    level the Griesmer cap leaves (9 for k_max = 14, 11 for 21), and
+    finalize_infoset."""
+    assert bench.launches_per_step(14, "auto") == 3 + 4 + 6 * 6
+    assert bench.launches_per_step(3, "auto") == 3 + 4
     assert bench.launches_per_step(14, "orbit") == 3
     assert bench.launches_per_step(1, "auto") == 3
-    assert bench.launches_per_step(21, "infoset") == 3 + 3 + 6 * 8
+    assert bench.launches_per_step(21, "infoset") == 3 + 4 + 6 * 8
