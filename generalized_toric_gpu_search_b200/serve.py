@@ -235,6 +235,101 @@ class ToricServer:
                     f.set_exception(exc)
 
 
+class ToricServerPool:
+    """One device-resident request loop per GPU behind one submit().
+
+    The reference spreads a batch over its GPUs with one host thread per
+    device (champion_search_canonical.py:237-271, mirrored by
+    distance.dispatch_max_zeros_batch).  For a stream of single requests each
+    device here runs its own persistent loop (a ToricServer), and every
+    request goes to the device with the fewest requests outstanding (ties to
+    the lowest index).  Codes are independent, so devices never exchange
+    data; the canonical dedup table is per device, so an equivalent request
+    routed to another device is evaluated again (the answer is the same).
+
+    `factory(device_id)` builds one server (ToricServer with the pool's
+    keyword arguments by default); it is a parameter so that the routing can
+    be exercised without GPUs.
+    """
+
+    def __init__(self, device_ids=None, *, factory=None, **server_kwargs):
+        if device_ids is None:
+            device_ids = list(range(torch.cuda.device_count()))
+        device_ids = list(device_ids)
+        if not device_ids:
+            raise ValueError("ToricServerPool needs at least one device")
+        if factory is None:
+            def factory(dev):
+                return ToricServer(dev, **server_kwargs)
+        self.device_ids = device_ids
+        self.servers = []
+        try:
+            for dev in device_ids:
+                self.servers.append(factory(dev))
+        except BaseException:
+            for srv in self.servers:
+                srv.close()
+            raise
+        self._lock = threading.Lock()
+        self._outstanding = [0] * len(self.servers)
+        self._owner: dict[int, int] = {}  # id(future) -> server index
+
+    def _release(self, i: int, fut: Future) -> None:
+        with self._lock:
+            self._outstanding[i] -= 1
+            self._owner.pop(id(fut), None)
+
+    def submit(self, indices, target_distance: int) -> Future:
+        """Queues one request on the least-loaded device; the future yields a
+        ServeAnswer (its id is the serving device's request id)."""
+        with self._lock:
+            i = min(range(len(self.servers)), key=lambda j: (self._outstanding[j], j))
+            self._outstanding[i] += 1
+        try:
+            fut = self.servers[i].submit(indices, target_distance)
+        except BaseException:
+            with self._lock:
+                self._outstanding[i] -= 1
+            raise
+        with self._lock:
+            self._owner[id(fut)] = i
+        fut.add_done_callback(lambda f, i=i: self._release(i, f))
+        return fut
+
+    def evaluate(self, requests, timeout: float = 600.0) -> list[ServeAnswer]:
+        """Submits (indices, target_distance) pairs and waits for all answers."""
+        futs = [self.submit(s, td) for s, td in requests]
+        return [f.result(timeout=timeout) for f in futs]
+
+    def cancel(self, fut: Future) -> bool:
+        """Cancels a request still waiting on its device's host queue."""
+        with self._lock:
+            i = self._owner.get(id(fut))
+        return False if i is None else self.servers[i].cancel(fut)
+
+    def outstanding(self) -> list[int]:
+        """Requests submitted and not yet answered, per device."""
+        with self._lock:
+            return list(self._outstanding)
+
+    def stats(self) -> dict:
+        """Per-device counters (ToricServer.stats) and their sums."""
+        per = [srv.stats() for srv in self.servers]
+        total = {k: sum(d[k] for d in per) for k in per[0] if k != "device_status"}
+        total["device_status"] = max(d.get("device_status", 0) for d in per)
+        return {"devices": dict(zip(self.device_ids, per)), "total": total}
+
+    def close(self) -> None:
+        for srv in self.servers:
+            srv.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
 class ToricBatchServer:
     """max_zeros requests served as continuous micro-batches of the batch path.
 

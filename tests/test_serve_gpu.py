@@ -135,3 +135,30 @@ def test_loop_relaunches_after_idle(gpu_oracle):
     assert a.passed and b.passed
     assert b.max_zeros == gpu_oracle.max_zeros_batch([s2], 1)[0]
     assert st["loop_launches"] >= 2
+
+
+def test_pool_of_every_visible_device_matches_batch(gpu_oracle):
+    """ToricServerPool over the visible GPUs (one here): each device runs its
+    own request loop, and the answers equal the batch oracle's."""
+    import torch
+
+    from generalized_toric_gpu_search_b200.serve import ToricServerPool
+
+    rng = random.Random(77)
+    reqs = [(sorted(rng.sample(range(N), rng.randint(8, 13))), rng.choice([1, 20, 24]))
+            for _ in range(24)]
+    exact = gpu_oracle.max_zeros_batch([s for s, _ in reqs], 1)
+    with ToricServerPool(k_max=13, max_slots=64, idle_us=3000, life_ms=100) as pool:
+        assert len(pool.servers) == torch.cuda.device_count()
+        got = pool.evaluate(reqs, timeout=300)
+        # done callbacks run in the servers' pump threads, just after the
+        # answers are delivered
+        import time
+
+        t_end = time.time() + 5.0
+        while any(pool.outstanding()) and time.time() < t_end:
+            time.sleep(0.01)
+        assert pool.outstanding() == [0] * len(pool.servers)
+        assert pool.stats()["total"]["finished"] == len(reqs)
+    for (s, td), a, e in zip(reqs, got, exact):
+        assert same_answer(a, e, td), (s, td, a, e)
