@@ -173,12 +173,22 @@ int tg_context_create(int device, const int32_t* h_M, tg_context** out_ctx) {
   ctx->device = device;
   ctx->sm_count = prop.multiProcessorCount;
   ctx->is_toric = std::memcmp(T, M, sizeof(M)) == 0 ? 1 : 0;
+  // The rows of M bit-sliced (one 49-bit word per GF(8) bit), as the
+  // information-set preparation loads them.
+  uint64_t planes[kN * 3] = {};
+  for (int r = 0; r < kN; ++r)
+    for (int j = 0; j < kN; ++j)
+      for (int b = 0; b < 3; ++b)
+        planes[r * 3 + b] |= uint64_t((M[r * kN + j] >> b) & 1u) << j;
   e = cudaMalloc(&ctx->d_M, sizeof(M));
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_Mp, sizeof(planes));
   if (e == cudaSuccess) e = cudaMalloc(&ctx->d_gl2, gl2.size());
   if (e == cudaSuccess) e = cudaMemcpy(ctx->d_M, M, sizeof(M), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(ctx->d_Mp, planes, sizeof(planes), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(ctx->d_gl2, gl2.data(), gl2.size(), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
     if (ctx->d_M) cudaFree(ctx->d_M);
+    if (ctx->d_Mp) cudaFree(ctx->d_Mp);
     if (ctx->d_gl2) cudaFree(ctx->d_gl2);
     delete ctx;
     return cuda_fail(e, "context tables");
@@ -191,6 +201,7 @@ int tg_context_destroy(tg_context* ctx) {
   if (!ctx) return TG_OK;
   DeviceGuard g(ctx->device);
   if (ctx->d_M) cudaFree(ctx->d_M);
+  if (ctx->d_Mp) cudaFree(ctx->d_Mp);
   if (ctx->d_gl2) cudaFree(ctx->d_gl2);
   delete ctx;
   return TG_OK;
@@ -305,6 +316,7 @@ static int bind_distance(tg_context* ctx, const tg_distance_params* p, const int
   a.sample_count = p->sample_count;
   a.seed = p->sample_seed;
   a.tab.M = ctx->d_M;
+  a.tab.Mp = ctx->d_Mp;
   a.tab.gl2 = ctx->d_gl2;
   a.is_toric = ctx->is_toric;
   a.is_blocks_per_sm = p->is_blocks_per_sm > 0 ? p->is_blocks_per_sm : 5;

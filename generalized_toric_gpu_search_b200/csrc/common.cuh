@@ -270,6 +270,7 @@ __device__ __forceinline__ void key_from_mask(uint64_t m, uint64_t& lo, uint64_t
 // Context tables shared by the kernels (device memory of one context).
 struct DeviceTables {
   const uint8_t* M;       // 49 x 49 matrix entries (row-major)
+  const uint64_t* Mp;     // 49 rows x 3 bit planes of M (bit j of plane b = bit b of M[row][j])
   const uint8_t* gl2;     // 2016 x 49 point permutations of GL2(F7)
 };
 

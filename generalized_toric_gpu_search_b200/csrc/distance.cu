@@ -384,6 +384,7 @@ prep_exact_kernel(DistArgs a) {
     a.abort[c] = 0;
     if (pr.n_tasks) {
       atomicAdd(&a.hdr->codewords, (unsigned long long)(pr.n_tasks * pow8(pr.R)));
+      a.hdr->has_tasks = 1;
     }
     if (ok && k > 0) atomicAdd(&a.hdr->ref_messages, double(pow8(k)) - 1.0);
   }
@@ -400,6 +401,16 @@ __global__ void __launch_bounds__(kScanThreads) scan_tasks_kernel(DistArgs a) {
   __shared__ int s_over;
   const int t = threadIdx.x;
   const int n = a.n;
+  if (a.hdr->has_tasks == 0) {
+    // No code has walk tasks (every set takes the information-set path, or
+    // none needs enumerating): the walks read no offset when the total is 0.
+    if (t == 0) {
+      a.task_off[n] = 0ull;
+      a.hdr->total_tasks = 0ull;
+      a.hdr->counter = 0ull;
+    }
+    return;
+  }
   if (t == 0) s_over = 0;
   const int chunk = (n + kScanThreads - 1) / kScanThreads;
   const int beg = min(n, t * chunk);
@@ -753,7 +764,10 @@ __global__ void __launch_bounds__(kPrepWarps * 32) prep_sampled_kernel(DistArgs 
     a.desc[c] = d;
     a.out[c] = result;
     a.abort[c] = 0;
-    if (n_tasks) atomicAdd(&a.hdr->codewords, (unsigned long long)a.sample_count);
+    if (n_tasks) {
+      atomicAdd(&a.hdr->codewords, (unsigned long long)a.sample_count);
+      a.hdr->has_tasks = 1;
+    }
   }
 }
 

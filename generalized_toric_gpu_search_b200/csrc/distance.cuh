@@ -8,7 +8,7 @@ namespace tg {
 // Workspace header (first 256 bytes of a distance workspace).
 struct WsHeader {
   int32_t status;                 // TG_OK or a TG_ERR_* raised on the device
-  int32_t pad0;
+  int32_t has_tasks;              // set by the prep kernels when some code has walk tasks
   unsigned long long counter;     // next unclaimed task
   unsigned long long total_tasks; // tasks of the run (after the scan)
   unsigned long long codewords;   // codewords the tasks cover

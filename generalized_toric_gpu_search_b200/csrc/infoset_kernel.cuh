@@ -199,12 +199,9 @@ __global__ void __launch_bounds__(kIsPrepWarps * 32) prep_infoset_kernel(DistArg
   if (k == 0) return;
   uint64_t o0 = 0ull, o1 = 0ull, o2 = 0ull;
   if (lane < k) {
-    for (int j = 0; j < kN; ++j) {
-      const uint64_t v = a.tab.M[my * kN + j];
-      o0 |= (v & 1ull) << j;
-      o1 |= ((v >> 1) & 1ull) << j;
-      o2 |= ((v >> 2) & 1ull) << j;
-    }
+    o0 = __ldg(a.tab.Mp + my * 3);
+    o1 = __ldg(a.tab.Mp + my * 3 + 1);
+    o2 = __ldg(a.tab.Mp + my * 3 + 2);
   }
   V6* base = a.is_rows + size_t(c) * a.is_stride;
   bool deficient = false;

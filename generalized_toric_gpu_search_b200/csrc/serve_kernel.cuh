@@ -221,12 +221,9 @@ __device__ void srv_evaluate(const SrvArgs& a, int lane, unsigned int slot, SrvS
   const int my = lane < k ? __ldcg(&h->idx[lane]) : 0;
   uint64_t p0 = 0ull, p1 = 0ull, p2 = 0ull;
   if (lane < k) {
-    for (int j = 0; j < kN; ++j) {
-      const uint64_t v = a.tab.M[my * kN + j];
-      p0 |= (v & 1ull) << j;
-      p1 |= ((v >> 1) & 1ull) << j;
-      p2 |= ((v >> 2) & 1ull) << j;
-    }
+    p0 = __ldg(a.tab.Mp + my * 3);
+    p1 = __ldg(a.tab.Mp + my * 3 + 1);
+    p2 = __ldg(a.tab.Mp + my * 3 + 2);
   }
   is_make_order(s_ord, 0, lane);
   uint64_t used = 0ull;

@@ -263,6 +263,7 @@ int tg_server_create(tg_context* ctx, const tg_server_params* p, void* d_arena,
   a.idle_ns = static_cast<unsigned long long>(q.idle_us) * 1000ull;
   a.life_ns = static_cast<unsigned long long>(q.life_ms) * 1000000ull;
   a.tab.M = ctx->d_M;
+  a.tab.Mp = ctx->d_Mp;
   a.tab.gl2 = ctx->d_gl2;
   e = cudaStreamCreateWithFlags(&srv->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&srv->aux, cudaStreamNonBlocking);
