@@ -46,11 +46,11 @@ POPC_PER_CODEWORD = 14.0 / 8.0  # histogram walk: 7 bins x 2 words per 8 codewor
 # codewords with 4 + 1 counts, so the executed POPC can be lower)
 POPC_PER_CODEWORD_INFOSET = 8.0 / 7.0
 # DRAM traffic of one walk_level_kernel launch (dram__bytes_read.sum +
-# dram__bytes_write.sum) from the ncu capture summarised in
-# profiles/walk_level_kernel_infoset_mixed_k.md: level 5 of 1000 sets of k = 14.
-# The walk reads each set's tables (7 x 32 B per row) and the task offsets;
-# it is integer-issue bound, and DRAM stays near idle.
-WALK_LEVEL5_DRAM_BYTES = 2.54e6
+# dram__bytes_write.sum) from an ncu capture of part 2 of level 5 of 1000 sets
+# of k = 14 (3.09e9 codewords).  The walk reads each set's tables (7 x 32 B
+# per row) and the task offsets; it is integer-issue bound, and DRAM stays
+# near idle.
+WALK_LEVEL5_DRAM_BYTES = 2.34e6
 
 
 # --enumeration: (TG_ENUM_* value, description)
@@ -996,7 +996,8 @@ def run_b200_arm(args, d: Dist) -> None:
             "roofline": {"bound": "int (POPC pipe)", "achieved": achieved / 1e12,
                          "peak": peak / 1e12, "unit": "Tpopc/s", "frac": achieved / peak,
                          "traffic": WALK_LEVEL5_DRAM_BYTES,
-                         "traffic_unit": "bytes per level-5 launch (ncu, 1000 sets of k = 14)",
+                         "traffic_unit": "bytes per launch of level 5 part 2 (ncu, 1000 "
+                                         "sets of k = 14, 3.09e9 codewords)",
                          "kernel": dominant["kernel"],
                          "kernel_share": dominant["seconds"] / (statistics.mean(step_ms) / 1e3),
                          "note": dominant["note"] + "; peak = measured POPC/clk/SM x SMs x "
