@@ -106,7 +106,7 @@ struct DistArgs {
   int is_max_task_units;         // largest task, in blocks
   IsHeader* is_hdr;              // task queue of the information-set walk
   V6* is_rows;                   // per code and set: k rows x (g, 6 deltas)
-  uint64_t* is_units;            // units of the current level per code
+  uint64_t* is_units;            // units of the current part per code position
   uint64_t* is_off;              // task offsets of the current level per code position (n + 1)
   int32_t* is_perm;              // code at each position (codes ordered by k)
   int32_t* is_best;              // smallest weight met per code

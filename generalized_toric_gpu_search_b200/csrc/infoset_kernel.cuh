@@ -376,10 +376,13 @@ __device__ __forceinline__ void is_part_supports(int32_t flags, int k, int w, in
 // Decides, with everything before part `part` (1 or 2) of level w complete,
 // whether each code is finished, and the units of that part for the others.
 __global__ void plan_level_kernel(DistArgs a, int w, int part) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  // One thread per code position (is_perm order): the units are written by
+  // position, so the scan and the walk read them in their own order.
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = p < a.n ? __ldg(a.is_perm + p) : 0;
   unsigned long long units = 0ull;
-  const CodeDesc d = c < a.n ? a.desc[c] : CodeDesc{};
-  if (c < a.n && (d.flags & kIsCodeFlag) != 0 && (d.flags & kDecidedFlag) == 0 &&
+  const CodeDesc d = p < a.n ? a.desc[c] : CodeDesc{};
+  if (p < a.n && (d.flags & kIsCodeFlag) != 0 && (d.flags & kDecidedFlag) == 0 &&
       a.abort[c] == 0 && (part == 1 || is_split_level(d.flags))) {
     const int best = a.is_best[c];
     bool done = w > d.k || best < kN - d.tmax;  // every message seen, or a witness
@@ -403,7 +406,7 @@ __global__ void plan_level_kernel(DistArgs a, int w, int part) {
       units = static_cast<unsigned long long>(d.H) * n_sup * is_units_per_support(w);
     }
   }
-  if (c < a.n) a.is_units[c] = units;
+  if (p < a.n) a.is_units[p] = units;
   // Lets scan_level_kernel and walk_level_kernel skip a part no set needs.
   if (__any_sync(0xffffffffu, units != 0ull) && (threadIdx.x & 31) == 0) a.is_hdr->work = 1;
 }
@@ -436,7 +439,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_level_kernel(DistArgs a, in
   unsigned long long sum = 0ull;
   bool over = false;
   for (int i = beg; i < end; ++i) {
-    const unsigned long long x = a.is_units[a.is_perm[i]];
+    const unsigned long long x = a.is_units[i];
     if (sum + x < sum) over = true;
     sum += x;
   }
@@ -480,7 +483,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_level_kernel(DistArgs a, in
   const unsigned long long nb = s_nb;
   // pass 2: tasks per code, exclusive scan
   unsigned long long tsum = 0ull;
-  for (int i = beg; i < end; ++i) tsum += (a.is_units[a.is_perm[i]] + nb - 1ull) / nb;
+  for (int i = beg; i < end; ++i) tsum += (a.is_units[i] + nb - 1ull) / nb;
   unsigned long long incl = tsum;
   for (int o = 1; o < 32; o <<= 1) {
     const unsigned long long y = __shfl_up_sync(0xffffffffu, incl, o);
@@ -501,7 +504,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_level_kernel(DistArgs a, in
   unsigned long long run = incl - tsum + (wid > 0 ? s_part[wid - 1] : 0ull);
   for (int i = beg; i < end; ++i) {
     a.is_off[i] = run;
-    run += (a.is_units[a.is_perm[i]] + nb - 1ull) / nb;
+    run += (a.is_units[i] + nb - 1ull) / nb;
   }
   __syncthreads();
   if (t == 0) {
@@ -1146,7 +1149,7 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) walk_level_kernel(DistArgs a
       } else {
         const unsigned long long u0 = (t - __ldg(a.is_off + p)) * nb;
         const unsigned long long u1 =
-            min(u0 + nb, static_cast<unsigned long long>(a.is_units[c]));
+            min(u0 + nb, static_cast<unsigned long long>(a.is_units[p]));
         unsigned long long ncw = 0ull;
         // Codewords no lighter than the code's best so far cannot change it,
         // so the walk starts from that best.
