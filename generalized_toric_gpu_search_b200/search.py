@@ -139,7 +139,8 @@ class CanonicalBFS:
             prune_eval_mode: str = "champion", screen_from_k: int | None = None,
             screen_sample_count: int = 0, screen_seed: int = 1, batch_size: int = 50_000,
             results_file: Path | str | None = None, resume: bool = True,
-            screen_candidate_log_limit: int = 200, lattice=None):
+            screen_candidate_log_limit: int = 200, lattice=None,
+            keys_file: Path | str | None = None):
         """Yields Level objects for the levels up to max_k, following
         canonical_champion_search (champion_search_canonical.py:386-604):
         per level k the target td = targets[k], keep distance and evaluation
@@ -148,14 +149,19 @@ class CanonicalBFS:
         else those with d >= keep distance) as the next level's parents.
         With results_file, the level's records are appended in the
         reference's JSONL format, and a run resumes after the last completed
-        level of that file (load_canonical_state)."""
+        level of that file (load_canonical_state).  With keys_file, each
+        level is also appended to a binary key stream (append_key_level);
+        without a results file, a run resumes from the key stream."""
         if prune_eval_mode not in ("champion", "survivor"):
             raise ValueError("prune_eval_mode must be 'champion' or 'survivor'")
         path = Path(results_file) if results_file is not None else None
+        keys_path = Path(keys_file) if keys_file is not None else None
         lattice = lattice if lattice is not None else bounding_cube_points()
         start_k, packed0 = 1, {0}
         if path is not None and resume and path.exists():
             start_k, packed0 = load_canonical_state(path)
+        elif keys_path is not None and resume and keys_path.exists():
+            start_k, packed0 = load_key_stream_state(keys_path)
         masks0 = sorted(mask_of(unpack_canonical(p, start_k)) for p in packed0)
         parents = torch.tensor(masks0, dtype=torch.int64, device=self.device)
         for k in range(start_k + 1, max_k + 1):
@@ -181,6 +187,12 @@ class CanonicalBFS:
                                         sample_count=sample_count,
                                         screen_candidate_log_limit=screen_candidate_log_limit)
                 append_records(recs, path)
+            if keys_path is not None:
+                h_masks, _, h_mz = lv.host()
+                kept = (np.ones(h_mz.shape, dtype=bool) if prune_margin is None
+                        else h_mz <= N_POINTS - keep_distance)
+                append_key_level(keys_path, k, h_masks, h_mz, kept, eval_distance=eval_distance,
+                                 keep_distance=keep_distance, screened=sample_count > 0)
             yield lv
             if prune_margin is None:
                 parents = lv.masks
@@ -303,3 +315,117 @@ def records(level: Level, best_known_d: int, prune_margin: int | None = None,
                            prune_eval_mode=prune_eval_mode, sample_count=sample_count,
                            eval_distance=level.eval_distance)
     return out
+
+
+# ---------------------------------------------------------------------------
+# Binary key stream (host side)
+# ---------------------------------------------------------------------------
+#
+# At high k the JSONL results file holds one survivor line per kept class
+# (about 40 bytes each, parsed line by line on resume).  The key stream keeps
+# the same facts in fixed-width little-endian arrays, one block per level:
+#
+#   file header   b"TGKS", uint32 version (1)
+#   level block   b"LEVL", int32 k, int32 flags (bit 0: values from sampled
+#                 screening), int64 n, int32 eval_distance,
+#                 int32 keep_distance, n x uint64 canonical masks,
+#                 n x int8 max_zeros, n x uint8 kept (survivor) flags,
+#                 b"DONE"
+#
+# A block without its closing b"DONE" (a run stopped while writing it) is
+# not a completed level: readers ignore it, as the JSONL reader ignores a
+# level without its level_complete record.  The JSONL file stays the
+# reference's format; the key stream is an addition next to it.
+
+KEYS_MAGIC = b"TGKS"
+KEYS_VERSION = 1
+_LEVEL_HEAD = np.dtype([("magic", "S4"), ("k", "<i4"), ("flags", "<i4"), ("n", "<i8"),
+                        ("eval_distance", "<i4"), ("keep_distance", "<i4")])
+
+
+@dataclass
+class KeyLevel:
+    """One completed level of a key stream."""
+
+    k: int
+    masks: np.ndarray        # (n,) uint64 canonical masks, evaluation order
+    max_zeros: np.ndarray    # (n,) int8
+    kept: np.ndarray         # (n,) bool, survivors for the next level
+    eval_distance: int
+    keep_distance: int
+    screened: bool
+
+
+def append_key_level(path: Path | str, k: int, masks, max_zeros, kept, *, eval_distance: int,
+                     keep_distance: int, screened: bool = False) -> None:
+    """Appends one level block (writing the file header first when the file
+    is new or empty)."""
+    masks = np.ascontiguousarray(np.asarray(masks).astype("<u8", copy=False))
+    mz = np.asarray(max_zeros)
+    if mz.size and (int(mz.min()) < 0 or int(mz.max()) > N_POINTS):
+        raise ValueError("max_zeros must lie in 0..49")
+    mz = np.ascontiguousarray(mz.astype("<i1"))
+    kept = np.ascontiguousarray(np.asarray(kept, dtype=bool).astype("<u1"))
+    if not (masks.shape == mz.shape == kept.shape) or masks.ndim != 1:
+        raise ValueError("masks, max_zeros and kept must be 1-D of one length")
+    head = np.zeros(1, dtype=_LEVEL_HEAD)
+    head[0] = (b"LEVL", k, 1 if screened else 0, masks.size, eval_distance, keep_distance)
+    path = Path(path)
+    new = not path.exists() or path.stat().st_size == 0
+    with path.open("ab") as f:
+        if new:
+            f.write(KEYS_MAGIC + np.uint32(KEYS_VERSION).astype("<u4").tobytes())
+        f.write(head.tobytes())
+        f.write(masks.tobytes())
+        f.write(mz.tobytes())
+        f.write(kept.tobytes())
+        f.write(b"DONE")
+
+
+def read_key_stream(path: Path | str) -> list[KeyLevel]:
+    """The completed levels of a key stream, in file order; a trailing
+    incomplete block is ignored.  Raises ValueError on a foreign file."""
+    data = Path(path).read_bytes()
+    if not data:
+        return []
+    if len(data) < 8 or data[:4] != KEYS_MAGIC:
+        raise ValueError(f"{path}: not a key stream")
+    version = int(np.frombuffer(data[4:8], dtype="<u4")[0])
+    if version != KEYS_VERSION:
+        raise ValueError(f"{path}: key stream version {version}, expected {KEYS_VERSION}")
+    out: list[KeyLevel] = []
+    pos, hs = 8, _LEVEL_HEAD.itemsize
+    while pos + hs <= len(data):
+        head = np.frombuffer(data[pos:pos + hs], dtype=_LEVEL_HEAD)[0]
+        if head["magic"] != b"LEVL":
+            raise ValueError(f"{path}: bad level block at byte {pos}")
+        n = int(head["n"])
+        end = pos + hs + 10 * n + 4
+        if n < 0 or end > len(data):
+            break  # incomplete block
+        body = pos + hs
+        masks = np.frombuffer(data[body:body + 8 * n], dtype="<u8").astype(np.uint64)
+        mz = np.frombuffer(data[body + 8 * n:body + 9 * n], dtype="<i1").copy()
+        kept = np.frombuffer(data[body + 9 * n:body + 10 * n], dtype="<u1").astype(bool)
+        if data[end - 4:end] != b"DONE":
+            break  # incomplete block
+        out.append(KeyLevel(int(head["k"]), masks, mz, kept, int(head["eval_distance"]),
+                            int(head["keep_distance"]), bool(int(head["flags"]) & 1)))
+        pos = end
+    return out
+
+
+def load_key_stream_state(path: Path | str) -> tuple[int, set[int]]:
+    """(last completed k, packed survivors of that level) of a key stream, or
+    (1, {0}) when it holds no completed level: the same answer
+    load_canonical_state gives for the JSONL file of the same run."""
+    path = Path(path)
+    levels = read_key_stream(path) if path.exists() else []
+    if not levels:
+        return 1, {0}
+    last = max(lv.k for lv in levels)
+    packed: set[int] = set()
+    for lv in levels:
+        if lv.k == last:
+            packed.update(pack_canonical(indices_of(int(m))) for m in lv.masks[lv.kept])
+    return last, packed
