@@ -7,6 +7,11 @@ hand-written sm_100a CUDA library:
   DistanceOracleCUDABP, init_cuda_oracles_bp   -- max_zeros / min distance
   CanonicalOracle, init_canon_oracle           -- AGL2(F7) canonical forms
   CanonicalDedup                               -- device hash-set dedup
+
+and the drivers built on them: ToricServer (device-resident request loop),
+ToricServerPool (one loop per GPU), ToricBatchServer (micro-batches of the
+batch path) and CanonicalBFS (the canonical search with every level on the
+GPU).
 """
 
 from .tables import (  # noqa: F401
@@ -32,6 +37,10 @@ __all__ = [
     "init_canon_oracle",
     "CanonicalDedup",
     "LaunchConfig",
+    "ToricServer",
+    "ToricServerPool",
+    "ToricBatchServer",
+    "CanonicalBFS",
     "build_eval_matrix",
     "precompute_gl2_perms",
     "rel_table",
@@ -51,4 +60,12 @@ def __getattr__(name):
         from . import canonical
 
         return getattr(canonical, name)
+    if name in ("ToricServer", "ToricServerPool", "ToricBatchServer", "ServeAnswer"):
+        from . import serve
+
+        return getattr(serve, name)
+    if name == "CanonicalBFS":
+        from . import search
+
+        return search.CanonicalBFS
     raise AttributeError(name)

@@ -1201,7 +1201,10 @@ __device__ int is_levels123_part(int tid, int nthr, const V6* base, int n_sets, 
   const int total = n_sets * per_set;
   const bool wit = wsrc.dst != nullptr;
   int wmin = kN + 1;
-  for (int u = tid; u < total; u += nthr) {
+  // Units from the last down: the 49-codeword triples first, the rows and
+  // pairs (1 and 7 codewords) last, where they even out the threads' loads.
+  for (int uu = tid; uu < total; uu += nthr) {
+    const int u = total - 1 - uu;
     const int j = u / per_set;
     int r = u - j * per_set;
     const V6* rows = base + size_t(j) * k * kIsVecPerRow;

@@ -65,23 +65,24 @@ def test_bfs_key_stream_matches_levels_and_resumes(tmp_path):
     """CanonicalBFS.run with keys_file writes each level's canonical masks,
     values and survivor flags to the binary key stream; a second run with
     only the key stream resumes after its last level and yields what an
-    uninterrupted run yields."""
+    uninterrupted run yields (every class kept, levels 2..7)."""
     from generalized_toric_gpu_search_b200.search import CanonicalBFS, read_key_stream
 
-    targets = {k: 49 - k + 1 - 3 for k in range(2, 8)}
+    targets = {k: 30 for k in range(2, 8)}
     keys = tmp_path / "keys.bin"
-    bfs = CanonicalBFS(0, dedup_capacity=1 << 22)
-    full = [lv.host() for lv in bfs.run(max_k=7, targets=targets, prune_margin=1)]
+    full = [lv.host() for lv in CanonicalBFS(0, dedup_capacity=1 << 22).run(
+        max_k=7, targets=targets)]
+    assert len(full) == 6
     first = [lv.host() for lv in CanonicalBFS(0, dedup_capacity=1 << 22).run(
-        max_k=5, targets=targets, prune_margin=1, keys_file=keys)]
+        max_k=5, targets=targets, keys_file=keys)]
     stream = read_key_stream(keys)
     assert [lv.k for lv in stream] == [2, 3, 4, 5]
     for (masks, _, mz), lv in zip(first, stream):
         assert np.array_equal(lv.masks, masks)
         assert np.array_equal(lv.max_zeros.astype(np.int32), mz)
-        assert np.array_equal(lv.kept, mz <= 49 - lv.keep_distance)
+        assert lv.kept.all() and lv.keep_distance == 1
     rest = [lv.host() for lv in CanonicalBFS(0, dedup_capacity=1 << 22).run(
-        max_k=7, targets=targets, prune_margin=1, keys_file=keys)]
+        max_k=7, targets=targets, keys_file=keys)]
     assert [len(r[0]) for r in rest] == [len(f[0]) for f in full[4:]]
     for (m_a, _, z_a), (m_b, _, z_b) in zip(rest, full[4:]):
         assert sorted(zip(m_a.tolist(), z_a.tolist())) == sorted(zip(m_b.tolist(), z_b.tolist()))
