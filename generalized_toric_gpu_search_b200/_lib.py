@@ -112,6 +112,10 @@ SIGNATURES: dict[str, tuple] = {
         c_int, [c_void_p, c_void_p, c_void_p, c_size_t, c_void_p, c_size_t, POINTER(c_void_p)]
     ),
     "tg_server_submit": (c_int, [c_void_p, c_void_p, c_int32, c_int32, POINTER(c_uint32)]),
+    "tg_server_submit_batch": (
+        c_int,
+        [c_void_p, c_void_p, c_void_p, c_int32, c_void_p, c_void_p, c_void_p, POINTER(c_int32)],
+    ),
     "tg_server_pump": (c_int, [c_void_p, POINTER(c_int32)]),
     "tg_server_poll": (c_int, [c_void_p, c_void_p, c_int32, POINTER(c_int32)]),
     "tg_server_stats": (c_int, [c_void_p, POINTER(c_uint64)]),

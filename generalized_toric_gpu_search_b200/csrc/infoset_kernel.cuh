@@ -460,7 +460,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_level_kernel(DistArgs a, in
     const unsigned long long target = static_cast<unsigned long long>(a.is_tasks_per_thread) *
                                       static_cast<unsigned long long>(a.is_lanes);
     unsigned long long nb = (tot + target - 1ull) / target;
-    // the largest task: the tunable limit from level 3 on (343 by default)
+    // the largest task: the tunable limit from level 3 on (49 by default)
     nb = max(1ull, min(nb, w >= 3 ? static_cast<unsigned long long>(a.is_max_task_units)
                                   : is_max_task_units(w)));
     // Align tasks with supports (units per support is a power of 7): whole

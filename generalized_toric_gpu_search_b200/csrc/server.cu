@@ -284,6 +284,9 @@ int tg_server_create(tg_context* ctx, const tg_server_params* p, void* d_arena,
   return TG_OK;
 }
 
+static int submit_locked(tg_server* srv, const int32_t* h_indices, int k, int target_distance,
+                         uint32_t* h_id);
+
 int tg_server_submit(tg_server* srv, const int32_t* h_indices, int32_t k, int32_t target_distance,
                      uint32_t* h_id) {
   if (!srv || (k > 0 && !h_indices)) {
@@ -301,6 +304,48 @@ int tg_server_submit(tg_server* srv, const int32_t* h_indices, int32_t k, int32_
     }
   }
   std::lock_guard<std::mutex> lock(srv->mu);
+  const int st = submit_locked(srv, h_indices, k, target_distance, h_id);
+  if (st == TG_OK) __atomic_store_n(&srv->h_ctl->published, srv->next_id, __ATOMIC_RELEASE);
+  return st;
+}
+
+int tg_server_submit_batch(tg_server* srv, const int32_t* h_indices, const int64_t* h_offsets,
+                           int32_t n, const int32_t* h_target, uint32_t* h_ids,
+                           int32_t* h_status, int32_t* h_consumed) {
+  if (!srv || n < 0 || (n > 0 && (!h_offsets || !h_target || !h_ids || !h_status)) ||
+      !h_consumed) {
+    set_last_error("tg_server_submit_batch: NULL argument or n < 0");
+    return TG_ERR_INVALID_ARGUMENT;
+  }
+  *h_consumed = 0;
+  std::lock_guard<std::mutex> lock(srv->mu);
+  int i = 0;
+  for (; i < n; ++i) {
+    const int64_t beg = h_offsets[i], len = h_offsets[i + 1] - beg;
+    int st = TG_OK;
+    if (len < 0 || len > srv->L.k_max || (len > 0 && !h_indices)) {
+      st = TG_ERR_INVALID_ARGUMENT;
+    } else {
+      for (int64_t j = 0; j < len; ++j)
+        if (h_indices[beg + j] < 0 || h_indices[beg + j] >= kN) st = TG_ERR_INVALID_ARGUMENT;
+    }
+    if (st == TG_OK) {
+      st = submit_locked(srv, len > 0 ? h_indices + beg : nullptr, int(len), h_target[i],
+                         h_ids + i);
+      if (st == TG_ERR_CAPACITY) break;  // this and later requests stay with the caller
+    }
+    h_status[i] = st;
+  }
+  *h_consumed = i;
+  // one publication store for the whole batch
+  __atomic_store_n(&srv->h_ctl->published, srv->next_id, __ATOMIC_RELEASE);
+  return TG_OK;
+}
+
+// Takes a free slot for one validated request and writes its publication
+// entry (the caller holds srv->mu and publishes the new count).
+static int submit_locked(tg_server* srv, const int32_t* h_indices, int k, int target_distance,
+                         uint32_t* h_id) {
   if (srv->free_slots.empty()) {
     set_last_error("all %d request slots are busy", srv->L.S);
     return TG_ERR_CAPACITY;
@@ -321,7 +366,6 @@ int tg_server_submit(tg_server* srv, const int32_t* h_indices, int32_t k, int32_
   srv->h_pubq[id % uint32_t(srv->L.Q)] =
       static_cast<unsigned long long>(uint32_t(slot)) | (static_cast<unsigned long long>(id) << 32);
   std::atomic_thread_fence(std::memory_order_release);
-  __atomic_store_n(&srv->h_ctl->published, id + 1u, __ATOMIC_RELEASE);
   srv->slot_id[slot] = id;
   srv->busy.push_back(slot);
   srv->busy_ids.push_back(id);

@@ -43,7 +43,7 @@ class LaunchConfig:
     blocks_per_sm: int = 0
     threads_per_block: int = 0
     # the information-set walk: CTAs per SM, tasks per resident thread of a
-    # level, largest task in 49-codeword blocks (0 = library defaults 5, 8, 343)
+    # level, largest task in 49-codeword blocks (0 = library defaults 5, 4, 49)
     is_blocks_per_sm: int = 0
     is_tasks_per_thread: int = 0
     is_max_task_units: int = 0

@@ -31,7 +31,7 @@ import threading
 import time
 from collections import deque
 from concurrent.futures import Future
-from dataclasses import dataclass
+from typing import NamedTuple
 
 import numpy as np
 import torch
@@ -41,9 +41,9 @@ from .distance import ToricContext
 from .tables import N_POINTS, build_eval_matrix
 
 
-@dataclass(frozen=True)
-class ServeAnswer:
-    """Answer of one served request."""
+class ServeAnswer(NamedTuple):
+    """Answer of one served request (a named tuple: a served burst builds
+    tens of thousands per second on the host)."""
 
     id: int
     max_zeros: int
@@ -94,34 +94,53 @@ class ToricServer:
         self._closed = False
         self._error: BaseException | None = None
         self._results = (_lib.ServerResult * 512)()
+        self._results_np = np.ctypeslib.as_array(self._results)  # a view of the same memory
+        self._slots_full = False  # the last admission stopped at a full pool
         self._thread = threading.Thread(target=self._pump_loop, name="toric-server", daemon=True)
         self._thread.start()
 
     # -- client API -----------------------------------------------------------
 
-    def submit(self, indices, target_distance: int) -> Future:
-        """Queues one request; the future yields a ServeAnswer."""
+    def _request(self, indices) -> np.ndarray:
         idx = np.ascontiguousarray(np.asarray(indices, dtype=np.int32).reshape(-1))
         if idx.size > self.k_max:
             raise ValueError(f"request has k = {idx.size} > k_max = {self.k_max}")
         if idx.size and (int(idx.min()) < 0 or int(idx.max()) >= N_POINTS):
             raise ValueError("exponent indices must lie in 0..48")
-        fut: Future = Future()
+        return idx
+
+    def _enqueue(self, items) -> None:
         with self._cv:
             if self._closed:
                 raise RuntimeError("server is closed")
             if self._error is not None:
                 raise RuntimeError("server failed") from self._error
-            if self.max_pending and len(self._pending) >= self.max_pending:
+            if self.max_pending and len(self._pending) + len(items) > self.max_pending:
                 raise _lib.ToricLibError(_lib.TG_ERR_CAPACITY,
                                          f"{len(self._pending)} requests already wait for a slot")
-            self._pending.append((idx, int(target_distance), fut, time.perf_counter()))
+            self._pending.extend(items)
             self._cv.notify()
+
+    def submit(self, indices, target_distance: int) -> Future:
+        """Queues one request; the future yields a ServeAnswer."""
+        idx = self._request(indices)
+        fut: Future = Future()
+        self._enqueue([(idx, int(target_distance), fut, time.perf_counter())])
         return fut
+
+    def submit_many(self, requests) -> list[Future]:
+        """Queues (indices, target_distance) pairs in one step (one lock and
+        one wake-up of the pump thread); one future per request, in order.
+        All or none are queued: a bad request or a full host queue raises
+        before any is."""
+        now = time.perf_counter()
+        items = [(self._request(s), int(td), Future(), now) for s, td in requests]
+        self._enqueue(items)
+        return [it[2] for it in items]
 
     def evaluate(self, requests, timeout: float = 600.0) -> list[ServeAnswer]:
         """Submits (indices, target_distance) pairs and waits for all answers."""
-        futs = [self.submit(s, td) for s, td in requests]
+        futs = self.submit_many(requests)
         return [f.result(timeout=timeout) for f in futs]
 
     def cancel(self, fut: Future) -> bool:
@@ -163,29 +182,54 @@ class ToricServer:
     # -- pump thread ----------------------------------------------------------
 
     def _admit(self) -> int:
-        """Moves waiting requests into free device slots."""
-        lib = self._lib
-        admitted = 0
-        rid = ctypes.c_uint32(0)
-        while True:
-            with self._cv:
-                if not self._pending:
-                    return admitted
-                idx, td, fut, t0 = self._pending[0]
-            st = lib.tg_server_submit(self.handle, idx.ctypes.data if idx.size else None,
-                                      idx.size, td, ctypes.byref(rid))
-            if st == _lib.TG_ERR_CAPACITY:
-                return admitted
-            with self._cv:
+        """Moves waiting requests into free device slots: the head of the
+        host queue (up to 1024 requests) in one tg_server_submit_batch call,
+        which takes them in order until the slots run out.  The queue's lock
+        is held throughout, so cancel() never races a request on its way to
+        the device."""
+        if self._slots_full:
+            return 0  # nothing can enter before an answer frees a slot
+        with self._cv:
+            if not self._pending:
+                return 0
+            batch = [self._pending[i] for i in range(min(len(self._pending), 1024))]
+            taken = self._submit_batch(batch)
+            for _ in range(taken):
                 self._pending.popleft()
+        self._slots_full = taken < len(batch)
+        admitted = 0
+        for i in range(taken):
+            _, _, fut, t0 = batch[i]
+            st, rid = self._batch_status[i], self._batch_ids[i]
             if st != _lib.TG_OK:
                 try:
-                    _lib.check(st, "tg_server_submit")
+                    _lib.check(int(st), "tg_server_submit_batch")
                 except BaseException as exc:  # noqa: BLE001 - delivered to the caller
                     fut.set_exception(exc)
                 continue
-            self._inflight[int(rid.value)] = (fut, t0)
+            self._inflight[int(rid)] = (fut, t0)
             admitted += 1
+        return admitted
+
+    def _submit_batch(self, batch) -> int:
+        """One tg_server_submit_batch call over `batch`; returns how many it
+        took (their statuses and ids in _batch_status / _batch_ids)."""
+        n = len(batch)
+        lens = np.fromiter((item[0].size for item in batch), dtype=np.int64, count=n)
+        offsets = np.zeros(n + 1, dtype=np.int64)
+        np.cumsum(lens, out=offsets[1:])
+        flat = (np.concatenate([item[0] for item in batch]) if offsets[-1]
+                else np.zeros(1, dtype=np.int32)).astype(np.int32, copy=False)
+        target = np.fromiter((item[1] for item in batch), dtype=np.int32, count=n)
+        ids = np.zeros(n, dtype=np.uint32)
+        status = np.zeros(n, dtype=np.int32)
+        consumed = ctypes.c_int32(0)
+        _lib.check(self._lib.tg_server_submit_batch(
+            self.handle, flat.ctypes.data, offsets.ctypes.data, n, target.ctypes.data,
+            ids.ctypes.data, status.ctypes.data, ctypes.byref(consumed)),
+            "tg_server_submit_batch")
+        self._batch_status, self._batch_ids = status, ids
+        return int(consumed.value)
 
     def _collect(self) -> int:
         lib = self._lib
@@ -193,19 +237,25 @@ class ToricServer:
         _lib.check(lib.tg_server_poll(self.handle, self._results, len(self._results),
                                       ctypes.byref(n)), "tg_server_poll")
         now = time.perf_counter()
-        for i in range(n.value):
-            r = self._results[i]
-            fut, t0 = self._inflight.pop(int(r.id))
-            flags = int(r.flags)
-            if flags & _lib.TG_RESULT_BAD_INPUT:
+        m = n.value
+        if not m:
+            return 0
+        self._slots_full = False
+        # the fields of all m results at once (one view, no per-field ctypes access)
+        res = self._results_np[:m]
+        ids, mzs, flags = res["id"].tolist(), res["max_zeros"].tolist(), res["flags"].tolist()
+        dev_s = ((res["t_done_ns"].astype(np.int64) - res["t_admit_ns"].astype(np.int64))
+                 * 1e-9).tolist()
+        bad, ok, dd = _lib.TG_RESULT_BAD_INPUT, _lib.TG_RESULT_PASS, _lib.TG_RESULT_DEDUP
+        for i in range(m):
+            fut, t0 = self._inflight.pop(ids[i])
+            fl = flags[i]
+            if fl & bad:
                 fut.set_exception(ValueError("request rejected by the device (bad input)"))
                 continue
-            fut.set_result(ServeAnswer(
-                id=int(r.id), max_zeros=int(r.max_zeros),
-                passed=bool(flags & _lib.TG_RESULT_PASS),
-                dedup=bool(flags & _lib.TG_RESULT_DEDUP), latency_s=now - t0,
-                device_s=(int(r.t_done_ns) - int(r.t_admit_ns)) / 1e9))
-        return n.value
+            fut.set_result(ServeAnswer(ids[i], mzs[i], bool(fl & ok), bool(fl & dd), now - t0,
+                                       dev_s[i]))
+        return m
 
     def _pump_loop(self) -> None:
         running = ctypes.c_int32(0)

@@ -121,9 +121,9 @@ typedef struct tg_distance_params {
   /* Launch shape of the information-set walk (ABI version 2): */
   int32_t is_blocks_per_sm;    /* CTAs of 128 threads per SM, 1..5; 0 = 5        */
   int32_t is_tasks_per_thread; /* a level is cut into about this many tasks per
-                                  resident thread, 1..64; 0 = 8                  */
+                                  resident thread, 1..64; 0 = 4                  */
   int32_t is_max_task_units;   /* largest task, in 49-codeword blocks, 1..2401;
-                                  0 = 343                                        */
+                                  0 = 49                                         */
   int32_t is_pad;
 } tg_distance_params;
 
@@ -372,6 +372,16 @@ int tg_server_create(tg_context* ctx, const tg_server_params* p, void* d_arena,
 /* Queues one request; TG_ERR_CAPACITY when every slot is busy. */
 int tg_server_submit(tg_server* srv, const int32_t* h_indices, int32_t k,
                      int32_t target_distance, uint32_t* h_id);
+/* Queues requests 0..n-1 in order (request i: h_indices[h_offsets[i] ..
+ * h_offsets[i+1]), threshold h_target[i]) under one lock and one publication
+ * store, until the slots run out.  *h_consumed = how many were taken from the
+ * front: h_status[i] is TG_OK (h_ids[i] = its id) or TG_ERR_INVALID_ARGUMENT
+ * (k or an index out of range; no id) for each of them; the rest stay with
+ * the caller.  Returns TG_OK, or TG_ERR_INVALID_ARGUMENT for bad pointers.
+ * No counterpart in the reference (its drivers evaluate batches). */
+int tg_server_submit_batch(tg_server* srv, const int32_t* h_indices, const int64_t* h_offsets,
+                           int32_t n, const int32_t* h_target, uint32_t* h_ids,
+                           int32_t* h_status, int32_t* h_consumed);
 /* (Re)launches the loop kernel when requests are outstanding and it has
  * exited; *h_running = 1 while a loop launch is executing. */
 int tg_server_pump(tg_server* srv, int32_t* h_running);

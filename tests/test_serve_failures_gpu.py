@@ -152,3 +152,23 @@ def test_missing_publication_times_out_and_the_loop_goes_on(gpu_oracle):
         st = srv.stats()
     assert st["device_status"] == _lib.TG_ERR_STATE
     assert st["published"] == 31 and st["finished"] == 30
+
+
+def test_submit_many_is_all_or_none(gpu_oracle):
+    """submit_many queues a list in one step or, when the host queue would
+    overflow or a request is malformed, queues none of it."""
+    from generalized_toric_gpu_search_b200 import _lib
+    from generalized_toric_gpu_search_b200.serve import ToricServer
+
+    rng = random.Random(9)
+    sets = [sorted(rng.sample(range(N), 12)) for _ in range(12)]
+    with ToricServer(0, k_max=15, max_slots=1, max_pending=6) as srv:
+        with pytest.raises(_lib.ToricLibError) as err:
+            srv.submit_many([(s, 1) for s in sets])
+        assert err.value.status == _lib.TG_ERR_CAPACITY
+        with pytest.raises(ValueError):
+            srv.submit_many([(sets[0], 1), ([0, 49], 1)])
+        assert srv.stats()["published"] == 0
+        futs = srv.submit_many([(s, 1) for s in sets[:5]])
+        _check([f.result(timeout=120) for f in futs], sets[:5],
+               gpu_oracle.max_zeros_batch(sets[:5], 1))
