@@ -570,7 +570,10 @@ __global__ void __launch_bounds__(kSrvTPB, kSrvPerSm) serve_kernel(SrvArgs a) {
     if (action < 0) break;
     was_idle = action == 0;
     if (action == 0) {
-      __nanosleep(20000);
+      // Idle warps poll the ring every ~80 us: shorter sleeps put their
+      // reads on the lines the busy warps claim from (p99 1.5 ms at 5-20 us,
+      // 1.0 ms at 40-80 us on the served stream, p50 unchanged).
+      __nanosleep(80000);
       continue;
     }
     arg = __shfl_sync(0xffffffffu, arg, 0);
