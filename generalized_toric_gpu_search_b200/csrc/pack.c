@@ -54,8 +54,13 @@ static int collect_batch(PyObject* batch, Batch* b) {
     return -1;
   }
   for (Py_ssize_t i = 0; i < b->n; ++i) {
-    b->inner[i] = PySequence_Fast(sets[i], "every set must be a sequence of indices");
-    if (!b->inner[i]) return -1;
+    if (PyList_CheckExact(sets[i]) || PyTuple_CheckExact(sets[i])) {
+      Py_INCREF(sets[i]);  /* already a fast sequence */
+      b->inner[i] = sets[i];
+    } else {
+      b->inner[i] = PySequence_Fast(sets[i], "every set must be a sequence of indices");
+      if (!b->inner[i]) return -1;
+    }
     const Py_ssize_t k = PySequence_Fast_GET_SIZE(b->inner[i]);
     b->total += k;
     if (k > b->k_max) b->k_max = k;
@@ -65,21 +70,33 @@ static int collect_batch(PyObject* batch, Batch* b) {
 
 /* Writes the flat indices and offsets; -1 with an exception set when an item
  * is not an int. */
+/* One item as a C long: exact ints that fit a machine word (every valid
+ * index) are read directly, anything else through PyLong_AsLong (which may
+ * call __index__). */
+static inline long item_value(PyObject* it) {
+#if PY_VERSION_HEX >= 0x030C0000
+  if (PyLong_CheckExact(it) && PyUnstable_Long_IsCompact((PyLongObject*)it))
+    return (long)PyUnstable_Long_CompactValue((PyLongObject*)it);
+#endif
+  return PyLong_AsLong(it);
+}
+
 static int fill_batch(const Batch* b, int32_t* f, int64_t* o, int* bad) {
   Py_ssize_t pos = 0;
-  *bad = 0;
+  int any_bad = 0;
   o[0] = 0;
   for (Py_ssize_t i = 0; i < b->n; ++i) {
     const Py_ssize_t k = PySequence_Fast_GET_SIZE(b->inner[i]);
     PyObject** items = PySequence_Fast_ITEMS(b->inner[i]);
     for (Py_ssize_t j = 0; j < k; ++j) {
-      const long v = PyLong_AsLong(items[j]);
+      const long v = item_value(items[j]);
       if (v == -1 && PyErr_Occurred()) return -1;
-      if (v < 0 || v > 48) *bad = 1;
+      any_bad |= (unsigned long)v > 48ul;
       f[pos++] = (v < INT32_MIN || v > INT32_MAX) ? -1 : (int32_t)v;
     }
     o[i + 1] = (int64_t)pos;
   }
+  *bad = any_bad;
   return 0;
 }
 
