@@ -173,58 +173,106 @@ __device__ __forceinline__ void mask_top_row(uint64_t m, int& t, uint32_t& bits)
   bits = uint32_t(m >> (7 * t)) & 0x7Fu;
 }
 
+// Smallest top row of the translates of an image with row occupancy R,
+// anchored at its points: the translation by -q moves row qa to row 0, and
+// the candidate's top row is the highest occupied row after that shift.
+__device__ __forceinline__ int min_top_row(uint32_t R) {
+  int tmin = 9;
+  for (uint32_t rows = R; rows != 0u; rows &= rows - 1u) {
+    const int qa = __ffs(rows) - 1;
+    const uint32_t rr = ((R >> qa) | (R << (7 - qa))) & 0x7Fu;
+    tmin = min(tmin, 31 - __clz(rr));
+  }
+  return tmin;
+}
+
 // AGL2(F7) canonical mask of S != 0 (the smallest mask among the images of S
-// that contain the origin), by one warp: lane l maps S by the matrices l, l + 32,
-// ... of the GL2 point table `perm` (2016 rows of 49 bytes; read through the
-// read-only path when kLdg), then translates each image by -q for every point
-// q of it.  A candidate's order is decided first by its top row and then by
-// that row's bits, which follow from the image's row occupancy R and one row
-// of the image, so candidates above the best so far are skipped without the
-// full translation.  The lanes share their best every 8 matrices.  Returns the
-// mask in every lane.
+// that contain the origin), by one warp.  A candidate's order is decided
+// first by its top row, then by that row's bits.
+//
+// Stage 1.  The image of point (x, y) under A = (a b; c d) lies in row
+// a x + b y: the row occupancy of A S, and so the smallest top row its
+// translates can reach, depend on A's first row only.  The table holds the
+// 2016 matrices in lexicographic order of (a, b, c, d), so each of the 48
+// first rows heads 42 consecutive matrices; the lanes take the 48 first rows
+// and find the smallest top row t* over all.
+//
+// Stage 2.  Only the matrices whose first row reaches t* can give the
+// minimum.  The lanes map S by those (lane l takes l, l + 32, ... of them,
+// from the table `perm`, read through the read-only path when kLdg), then
+// translate each image by -q for every point q of its rows that reach t*;
+// candidates above the best so far are skipped on their top-row bits without
+// the full translation.  The lanes share their best every 8 matrices.
+// Returns the mask in every lane.
 // kRow: bytes between the table's rows (49 in global memory; the shared copy
 // pads rows to 52 bytes, a 13-word stride that keeps the lanes' loads on
 // distinct banks).
 template <bool kLdg, int kRow = kN>
 __device__ __forceinline__ uint64_t canon_mask_warp_min(int lane, uint64_t S,
                                                          const uint8_t* perm) {
-  uint64_t best = ~0ull;
-  int tb = 9;           // best's top row (9: none yet)
-  uint32_t pb = 0x7Fu;  // best's top-row bits
-  for (int A = lane, it = 0; A < kGl2Order; A += 32, ++it) {
-    const uint8_t* P = perm + A * kRow;
-    uint64_t img = 0ull;
-    uint32_t R = 0u;
-    uint64_t x = S;
-    while (x) {
-      const int p = __ffsll(static_cast<long long>(x)) - 1;
-      x &= x - 1ull;
-      const int idx = kLdg ? __ldg(P + p) : P[p];
-      img |= 1ull << idx;
-      R |= 1u << ((idx * 37) >> 8);  // row idx / 7
+  constexpr int kGroups = kGl2Order / 42;  // first rows (a, b) != (0, 0)
+  int tg[2] = {9, 9};
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int g = lane + 32 * h;
+    if (g < kGroups) {
+      const uint8_t* P = perm + g * 42 * kRow;
+      uint32_t R = 0u;
+      for (uint64_t x = S; x != 0ull; x &= x - 1ull) {
+        const int p = __ffsll(static_cast<long long>(x)) - 1;
+        const int idx = kLdg ? __ldg(P + p) : P[p];
+        R |= 1u << ((idx * 37) >> 8);  // row idx / 7
+      }
+      tg[h] = min_top_row(R);
     }
-    // Anchors q = (qa, qb) row by row: the rows after the shift, and so the
-    // top row t and the image row ra that lands on it, depend on qa only.
-    for (uint32_t rows = R; rows != 0u; rows &= rows - 1u) {
-      const int qa = __ffs(rows) - 1;
-      const uint32_t rr = ((R >> qa) | (R << (7 - qa))) & 0x7Fu;  // rows after the shift
-      const int t = 31 - __clz(rr);
-      if (t > tb) continue;
-      int ra = qa + t;
-      ra = ra >= 7 ? ra - 7 : ra;
-      const uint32_t rb = uint32_t(img >> (7 * ra)) & 0x7Fu;
-      for (uint32_t cols = uint32_t(img >> (7 * qa)) & 0x7Fu; cols != 0u; cols &= cols - 1u) {
-        const int qb = __ffs(cols) - 1;
-        // t <= tb here; an improvement makes tb = t
-        if (t == tb && (((rb >> qb) | (rb << (7 - qb))) & 0x7Fu) > pb) continue;
-        const uint64_t cand = torus_shift(img, qa, qb);
-        if (cand < best) {
-          best = cand;
-          mask_top_row(best, tb, pb);
+  }
+  int tstar = min(tg[0], tg[1]);
+  for (int o = 16; o > 0; o >>= 1) tstar = min(tstar, __shfl_xor_sync(0xffffffffu, tstar, o));
+  const unsigned cand0 = __ballot_sync(0xffffffffu, tg[0] == tstar);
+  const unsigned cand1 = __ballot_sync(0xffffffffu, tg[1] == tstar) & 0xFFFFu;  // groups 32..47
+  const int n0 = __popc(cand0);
+  const int n_mat = 42 * (n0 + __popc(cand1));
+
+  uint64_t best = ~0ull;
+  int tb = tstar;       // no candidate can have a lower top row
+  uint32_t pb = 0x7Fu;  // best's top-row bits (none yet)
+  for (int j = lane, it = 0; j - lane < n_mat; j += 32, ++it) {
+    if (j < n_mat) {
+      // the (j / 42)-th candidate first row, matrix j % 42 of its group
+      const int q = j / 42;
+      const int g = q < n0 ? __fns(cand0, 0, q + 1) : 32 + __fns(cand1, 0, q - n0 + 1);
+      const uint8_t* P = perm + (g * 42 + (j - 42 * q)) * kRow;
+      uint64_t img = 0ull;
+      uint32_t R = 0u;
+      for (uint64_t x = S; x != 0ull; x &= x - 1ull) {
+        const int p = __ffsll(static_cast<long long>(x)) - 1;
+        const int idx = kLdg ? __ldg(P + p) : P[p];
+        img |= 1ull << idx;
+        R |= 1u << ((idx * 37) >> 8);  // row idx / 7
+      }
+      // Anchors q = (qa, qb) row by row: the rows after the shift, and so the
+      // top row t and the image row ra that lands on it, depend on qa only.
+      for (uint32_t rows = R; rows != 0u; rows &= rows - 1u) {
+        const int qa = __ffs(rows) - 1;
+        const uint32_t rr = ((R >> qa) | (R << (7 - qa))) & 0x7Fu;  // rows after the shift
+        const int t = 31 - __clz(rr);
+        if (t > tb) continue;
+        int ra = qa + t;
+        ra = ra >= 7 ? ra - 7 : ra;
+        const uint32_t rb = uint32_t(img >> (7 * ra)) & 0x7Fu;
+        for (uint32_t cols = uint32_t(img >> (7 * qa)) & 0x7Fu; cols != 0u; cols &= cols - 1u) {
+          const int qb = __ffs(cols) - 1;
+          // t == tb here (tb is already the smallest possible top row)
+          if ((((rb >> qb) | (rb << (7 - qb))) & 0x7Fu) > pb) continue;
+          const uint64_t cand = torus_shift(img, qa, qb);
+          if (cand < best) {
+            best = cand;
+            mask_top_row(best, tb, pb);
+          }
         }
       }
     }
-    if ((it & 7) == 7 || A + 32 >= kGl2Order) {  // every lane runs 63 matrices
+    if ((it & 7) == 7 || j + 32 - lane >= n_mat) {
       uint64_t m = best;
       for (int o = 16; o > 0; o >>= 1) {
         const uint64_t other = __shfl_xor_sync(0xffffffffu, m, o);
