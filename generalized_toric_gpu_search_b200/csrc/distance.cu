@@ -935,10 +935,11 @@ int run_walk(const DistArgs& args, int sm_count, int blocks_per_sm, int tpb, cud
   }
   if (e != cudaSuccess) return cuda_fail(e, "walk kernel launch");
   if ((parts & kWalkInfoset) && args.is_min_k <= args.k_max) {
-    // Information-set walk, one level per launch triple; 5 CTAs of 128
-    // threads per SM (96 registers, no spills, 28 KB of shared memory each;
-    // 6 CTAs at 80 registers spill and ran 1 % slower).  Levels no code needs
-    // return before any setup.
+    // Information-set walk: levels 1 to 3 in one launch, then a plan / scan /
+    // walk triple per part of each level; 5 CTAs of 128 threads per SM for
+    // the walk (96 registers, no spills, 28 KB of shared memory each; 6 CTAs
+    // at 80 registers spill and ran 1 % slower).  Parts no code needs return
+    // before any setup.
     constexpr int kPerSm = 5;  // register budget of the walk (96 per thread)
     DistArgs la = args;
     const int per_sm = args.is_blocks_per_sm > 0 ? min(args.is_blocks_per_sm, kPerSm) : kPerSm;
