@@ -570,7 +570,7 @@ int tg_distance_stage_counters(const tg_distance_params* p, const void* d_worksp
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_fail(e, "tg_distance_stage_counters");
   }
-  // Levels 1 to 3 add to the total only (one warp per set; no second atomic).
+  // Levels 1 to 3 add to the total only (one CTA per set; no second atomic).
   unsigned long long later = 0ull;
   for (int i = 1; i < kIsStages; ++i) later += hi.stage_codewords[i];
   hi.stage_codewords[0] = hi.codewords - later;

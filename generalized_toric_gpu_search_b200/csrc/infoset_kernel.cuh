@@ -20,12 +20,13 @@
 // one broadcast; each set's columns are reordered with the pivots last (in
 // the high word).
 //
-// Levels 1 to 3 run as one warp-per-set launch (levels123_kernel).  From level
-// 4 on, each level is a launch triple: plan_level_kernel finishes the codes
-// whose bound is met and sizes the level for the others, scan_level_kernel
+// Levels 1 to 3 run as one launch (levels123_kernel, one CTA per set).  From
+// level 4 on, each level runs in two parts (supports with the set's last row,
+// then the rest), each a launch triple: plan_level_kernel finishes the codes
+// whose bound is met and sizes the part for the others, scan_level_kernel
 // picks the task size and the offsets, and walk_level_kernel hands the tasks
-// to a persistent grid.  No code starts a level before the previous one is
-// complete, so no work is spent on levels a code turns out not to need.
+// to a persistent grid.  No code starts a part before the previous one is
+// complete, so no work is spent on parts a code turns out not to need.
 //
 // Walk.  A support of w rows has its last row at coefficient 1.  A block is 49
 // codewords: digit 0 swept through its 7 multiples, digit 1 stepping
