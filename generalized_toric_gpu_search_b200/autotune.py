@@ -76,7 +76,9 @@ def save_table(device_name: str, table: dict[int, dict], path: Path | None = Non
         except (OSError, ValueError):
             doc = {}
     doc[device_name] = {str(k): v for k, v in sorted(table.items())}
-    tmp = p.with_suffix(".tmp")
+    # One temporary file per process: ranks of a multi-GPU run tune and save
+    # at the same time, and each rename installs a complete file.
+    tmp = p.with_suffix(f".{os.getpid()}.tmp")
     tmp.write_text(json.dumps(doc, indent=1, sort_keys=True))
     os.replace(tmp, p)
     return p
