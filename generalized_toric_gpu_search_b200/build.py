@@ -51,7 +51,7 @@ def build(force: bool = False, ptxas_verbose: bool = False) -> Path:
         "-fPIC,-O2",
         "-shared",
         "-o",
-        str(LIB_PATH) + ".tmp",
+        str(LIB_PATH) + f".{os.getpid()}.tmp",
         *[str(CSRC / s) for s in SOURCES],
     ]
     if ptxas_verbose:
@@ -63,7 +63,8 @@ def build(force: bool = False, ptxas_verbose: bool = False) -> Path:
         )
     if ptxas_verbose:
         sys.stderr.write(proc.stderr)
-    os.replace(str(LIB_PATH) + ".tmp", LIB_PATH)
+    # a per-process temporary name: ranks started together may build at once
+    os.replace(str(LIB_PATH) + f".{os.getpid()}.tmp", LIB_PATH)
     return LIB_PATH
 
 
@@ -86,11 +87,11 @@ def build_pack(force: bool = False) -> Path:
     if cc is None:
         raise RuntimeError("no C compiler found for the batch packer")
     cmd = [cc, "-O2", "-shared", "-fPIC", "-I" + sysconfig.get_paths()["include"], str(src),
-           "-o", str(out) + ".tmp"]
+           "-o", str(out) + f".{os.getpid()}.tmp"]
     proc = subprocess.run(cmd, capture_output=True, text=True)
     if proc.returncode != 0:
         raise RuntimeError("packer build failed:\n%s\n%s" % (" ".join(cmd), proc.stderr))
-    os.replace(str(out) + ".tmp", out)
+    os.replace(str(out) + f".{os.getpid()}.tmp", out)
     return out
 
 

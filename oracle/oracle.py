@@ -30,7 +30,7 @@ def build(force: bool = False) -> Path:
     """gcc -O3 -fopenmp build of the C restatement (portable x86-64-v3)."""
     if not force and LIB.exists() and LIB.stat().st_mtime >= SRC.stat().st_mtime:
         return LIB
-    tmp = str(LIB) + ".tmp"
+    tmp = str(LIB) + f".{os.getpid()}.tmp"  # processes started together may build at once
     cmd = ["gcc", "-O3", "-march=x86-64-v3", "-fopenmp", "-fPIC", "-shared", "-o", tmp,
            str(SRC)]
     proc = subprocess.run(cmd, capture_output=True, text=True)
