@@ -149,7 +149,13 @@ def test_missing_publication_times_out_and_the_loop_goes_on(gpu_oracle):
         assert srv.stats()["device_status"] == 0
         _lib.check(_lib.load().tg_server_debug_skip_publication(srv.handle), "skip")
         _check(srv.evaluate([(s, 1) for s in sets[10:]], timeout=120), sets[10:], exact[10:])
+        # The later requests may all be answered before the wait for the
+        # missing entry (a few milliseconds) runs out: poll the status.
+        deadline = time.time() + 5.0
         st = srv.stats()
+        while st["device_status"] == 0 and time.time() < deadline:
+            time.sleep(0.002)
+            st = srv.stats()
     assert st["device_status"] == _lib.TG_ERR_STATE
     assert st["published"] == 31 and st["finished"] == 30
 
@@ -172,3 +178,57 @@ def test_submit_many_is_all_or_none(gpu_oracle):
         futs = srv.submit_many([(s, 1) for s in sets[:5]])
         _check([f.result(timeout=120) for f in futs], sets[:5],
                gpu_oracle.max_zeros_batch(sets[:5], 1))
+
+
+def test_batch_submission_through_the_c_abi(M, gpu_oracle):
+    """tg_server_submit_batch takes requests in order under one lock: a
+    malformed one gets its own error status and no id, the slots' end stops
+    the batch (the rest stay with the caller), and every accepted request
+    gets the batch oracle's answer."""
+    import torch
+
+    from generalized_toric_gpu_search_b200 import _lib
+    from generalized_toric_gpu_search_b200.distance import ToricContext
+
+    lib = _lib.load()
+    ctx = ToricContext(0, M)
+    p = _lib.ServerParams(max_slots=3, k_max=12, table_capacity=-1)
+    slots, dev_b, host_b = ctypes.c_int32(0), ctypes.c_size_t(0), ctypes.c_size_t(0)
+    _lib.check(lib.tg_server_layout(ctx.handle, ctypes.byref(p), ctypes.byref(slots),
+                                    ctypes.byref(dev_b), ctypes.byref(host_b)), "layout")
+    arena = torch.empty(int(dev_b.value), dtype=torch.uint8, device="cuda")
+    host = torch.empty(int(host_b.value), dtype=torch.uint8, pin_memory=True)
+    h = ctypes.c_void_p()
+    _lib.check(lib.tg_server_create(ctx.handle, ctypes.byref(p), arena.data_ptr(), arena.numel(),
+                                    host.data_ptr(), host.numel(), ctypes.byref(h)), "create")
+    rng = random.Random(21)
+    good = [sorted(rng.sample(range(N), 9)) for _ in range(4)]
+    reqs = [good[0], [3, 60, 7], good[1], good[2], good[3]]  # the second is malformed
+    flat = np.array([i for s in reqs for i in s], dtype=np.int32)
+    offs = np.zeros(len(reqs) + 1, dtype=np.int64)
+    offs[1:] = np.cumsum([len(s) for s in reqs])
+    td = np.ones(len(reqs), dtype=np.int32)
+    ids = np.zeros(len(reqs), dtype=np.uint32)
+    st = np.full(len(reqs), 99, dtype=np.int32)
+    consumed = ctypes.c_int32(-1)
+    _lib.check(lib.tg_server_submit_batch(h, flat.ctypes.data, offs.ctypes.data, len(reqs),
+                                          td.ctypes.data, ids.ctypes.data, st.ctypes.data,
+                                          ctypes.byref(consumed)), "submit_batch")
+    # three slots: good[0], the malformed one (no slot), good[1], good[2]; good[3] waits
+    assert consumed.value == 4
+    assert st[:4].tolist() == [0, _lib.TG_ERR_INVALID_ARGUMENT, 0, 0]
+    want = dict(zip([int(ids[0]), int(ids[2]), int(ids[3])],
+                    gpu_oracle.max_zeros_batch([good[0], good[1], good[2]], 1)))
+    out = (_lib.ServerResult * 4)()
+    got = {}
+    running = ctypes.c_int32(0)
+    deadline = time.time() + 60
+    while len(got) < 3 and time.time() < deadline:
+        _lib.check(lib.tg_server_pump(h, ctypes.byref(running)), "pump")
+        n = ctypes.c_int32(0)
+        _lib.check(lib.tg_server_poll(h, out, 4, ctypes.byref(n)), "poll")
+        for i in range(n.value):
+            got[int(out[i].id)] = int(out[i].max_zeros)
+        time.sleep(0.001)
+    assert got == want
+    _lib.check(lib.tg_server_destroy(h), "destroy")
