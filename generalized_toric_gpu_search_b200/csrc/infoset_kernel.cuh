@@ -142,6 +142,44 @@ __device__ int is_gauss_jordan(int lane, int k, uint64_t& p0, uint64_t& p1, uint
   return rank;
 }
 
+// Move masks of a bit compress (gather the bits of x selected by m to the low
+// end, in order): six rounds, round i shifting some bits right by 2^i (the
+// parallel-suffix method of Hacker's Delight, 7-4).  They depend on m only.
+struct IsCompress {
+  uint64_t m;
+  uint64_t mv[6];
+};
+
+__device__ __forceinline__ IsCompress is_compress_masks(uint64_t m) {
+  IsCompress c;
+  c.m = m;
+  uint64_t mk = ~m << 1;  // the zeros of m to the right of each bit
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+    uint64_t mp = mk ^ (mk << 1);  // parity of those zeros, by a prefix XOR
+    mp ^= mp << 2;
+    mp ^= mp << 4;
+    mp ^= mp << 8;
+    mp ^= mp << 16;
+    mp ^= mp << 32;
+    const uint64_t mv = mp & m;  // bits that move by 2^i this round
+    c.mv[i] = mv;
+    m = (m ^ mv) | (mv >> (1 << i));
+    mk &= ~mp;
+  }
+  return c;
+}
+
+__device__ __forceinline__ uint64_t is_compress(uint64_t x, const IsCompress& c) {
+  x &= c.m;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+    const uint64_t t = x & c.mv[i];
+    x = (x ^ t) | (t >> (1 << i));
+  }
+  return x;
+}
+
 // Reorders the 49 columns of a bit-sliced row: the columns outside `piv`
 // first (increasing), then those in `piv`.  Weights do not depend on the
 // column order, and a set's codewords are sparse on its own pivot columns;
@@ -149,22 +187,14 @@ __device__ int is_gauss_jordan(int lane, int k, uint64_t& p0, uint64_t& p1, uint
 // low-half weight bound is tight.
 __device__ __forceinline__ void is_reorder_columns(uint64_t piv, uint64_t& p0, uint64_t& p1,
                                                    uint64_t& p2) {
-  uint64_t q0 = 0ull, q1 = 0ull, q2 = 0ull;
-  uint64_t rest = ~piv & kMask49;
-  uint64_t tail = piv & kMask49;
-  for (int d = 0; d < kN; ++d) {
-    const bool front = rest != 0ull;
-    const uint64_t pick = front ? rest : tail;
-    const int col = __ffsll(static_cast<long long>(pick)) - 1;
-    if (front) rest &= rest - 1ull;
-    else tail &= tail - 1ull;
-    q0 |= ((p0 >> col) & 1ull) << d;
-    q1 |= ((p1 >> col) & 1ull) << d;
-    q2 |= ((p2 >> col) & 1ull) << d;
-  }
-  p0 = q0;
-  p1 = q1;
-  p2 = q2;
+  // The non-pivot columns in increasing order, then the pivot columns.
+  const uint64_t rest = ~piv & kMask49;
+  const IsCompress cr = is_compress_masks(rest);
+  const IsCompress cp = is_compress_masks(piv & kMask49);
+  const int nr = __popcll(rest);
+  p0 = is_compress(p0, cr) | (is_compress(p0, cp) << nr);
+  p1 = is_compress(p1, cr) | (is_compress(p1, cp) << nr);
+  p2 = is_compress(p2, cr) | (is_compress(p2, cp) << nr);
 }
 
 // Writes the rows of one set: g and the six Gray-step deltas per row.
