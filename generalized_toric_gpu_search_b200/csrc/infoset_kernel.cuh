@@ -819,6 +819,16 @@ __device__ __forceinline__ int is_sweep_fix(uint32_t kC, const int (&z)[7], int 
       thz = thz_base - wmin;                                                                     \
     }                                                                                            \
   }
+// The same single-count test with the flagged sweeps counted after the
+// block (bit S of fl), so the block is one stretch of straight-line code.
+#define TG_IS_SWEEP1F(S)                                                                         \
+  {                                                                                              \
+    TG_IS_ZCOUNTS(z_)                                                                            \
+    const int pz_ = __popc(lop3<0xFE>(Pz.x0, Pz.x1, Pz.x2));                                    \
+    const int zm_ = __vimax3_s32(__vimax3_s32(z_[0], z_[1], z_[2]),                              \
+                                 __vimax3_s32(z_[3], z_[4], z_[5]), z_[6]) - pz_;                \
+    fl |= zm_ > thz ? (1u << (S)) : 0u;                                                          \
+  }
 // The same test on pairs of codewords: the selections of alpha^0|alpha^1,
 // alpha^2|alpha^3 and alpha^4|alpha^5 are disjoint, so each pair's count
 // bounds both of its codewords' zeros; four counts instead of seven.  Used at
@@ -881,6 +891,15 @@ __device__ __forceinline__ int is_block_fix(unsigned fl, Pl3 W, Pl3 Pz, const ui
 // hold a flagged sweep, and counting it leaves the other lanes idle: single
 // counts there made C2 0.9 % faster.
 constexpr int kIsPairThr = 16;
+// Smallest thr at which single counts are flagged and counted after the block
+// rather than on the spot.  A single count tops 10 in about 0.1 % of the
+// codewords, so few blocks hold a flag; below that, stepping back through
+// digit 1's moves to a flagged sweep costs more than a branch per sweep.  On
+// the mixed-k batch the straight-line blocks made the step 0.3 % faster (the
+// 14-row codes, at thr 14 and 15 on level 4, 4.5 %; the 12-row codes, at
+// thr 11 to 13, 1.2 % slower); starting them at 13 or 14 instead was slower
+// for all three.
+constexpr int kIsDeferThr = 10;
 
 // Walks blocks [b0, b0 + nblk) of one support; P is the sum of its rows other
 // than digit 0 at the start of block b0.  Each block is 7 sweeps of digit 0
@@ -976,6 +995,10 @@ __device__ __forceinline__ unsigned long long is_walk_blocks(
       TG_IS_SWEEP2(0); TG_IS_MOVE(0); TG_IS_SWEEP2(1); TG_IS_MOVE(1); TG_IS_SWEEP2(2);
       TG_IS_MOVE(2); TG_IS_SWEEP2(3); TG_IS_MOVE(3); TG_IS_SWEEP2(4); TG_IS_MOVE(4);
       TG_IS_SWEEP2(5); TG_IS_MOVE(5); TG_IS_SWEEP2(6);
+    } else if (thz + ngz >= kIsDeferThr) {
+      TG_IS_SWEEP1F(0); TG_IS_MOVE(0); TG_IS_SWEEP1F(1); TG_IS_MOVE(1); TG_IS_SWEEP1F(2);
+      TG_IS_MOVE(2); TG_IS_SWEEP1F(3); TG_IS_MOVE(3); TG_IS_SWEEP1F(4); TG_IS_MOVE(4);
+      TG_IS_SWEEP1F(5); TG_IS_MOVE(5); TG_IS_SWEEP1F(6);
     } else {
       TG_IS_SWEEP1(0, 1u); TG_IS_MOVE(0); TG_IS_SWEEP1(1, 2u); TG_IS_MOVE(1); TG_IS_SWEEP1(2, 4u);
       TG_IS_MOVE(2); TG_IS_SWEEP1(3, 3u); TG_IS_MOVE(3); TG_IS_SWEEP1(4, 6u); TG_IS_MOVE(4);
@@ -996,6 +1019,7 @@ __device__ __forceinline__ unsigned long long is_walk_blocks(
 
 #undef TG_IS_MOVE
 #undef TG_IS_SWEEP2
+#undef TG_IS_SWEEP1F
 #undef TG_IS_SWEEP1
 #undef TG_IS_ZCOUNTS
 
