@@ -320,7 +320,8 @@ static int bind_distance(tg_context* ctx, const tg_distance_params* p, const int
   a.tab.gl2 = ctx->d_gl2;
   a.is_toric = ctx->is_toric;
   a.is_blocks_per_sm = p->is_blocks_per_sm > 0 ? p->is_blocks_per_sm : 5;
-  // defaults: the shape the tuner picks for C2's largest codes (k = 14)
+  // defaults: the shape the tuner picks for k = 14, the largest codes of a
+  // batch of 10,000 sets with k from 6 to 14
   a.is_tasks_per_thread = p->is_tasks_per_thread > 0 ? p->is_tasks_per_thread : 4;
   a.is_max_task_units = p->is_max_task_units > 0 ? p->is_max_task_units : 49;
   bind_workspace(a, L, d_workspace);

@@ -347,7 +347,8 @@ __device__ __forceinline__ unsigned long long is_max_task_units(int w) {
 // Orders the codes by k for the level walks (is_perm: position -> code).
 // Tasks are numbered over positions, so where a warp's 32 tasks span two
 // codes those have the same k, the same loop lengths and, mostly, the same
-// threshold mode (in batch order, with k mixed, C2 ran 3 % slower).  One CTA;
+// threshold mode (in batch order, a batch of 10,000 sets with k from 6 to 14
+// ran 3 % slower).  One CTA;
 // the order within a k is that of the atomics (it changes no result).
 __global__ void __launch_bounds__(kScanThreads) order_codes_kernel(DistArgs a) {
   __shared__ int s_cnt[kIsBinom + 1];
@@ -889,16 +890,16 @@ __device__ __forceinline__ int is_block_fix(unsigned fl, Pl3 W, Pl3 Pz, const ui
 // in about 0.3 % of the sweeps and 16 in about 0.08 %, against 1.3e-5 for the
 // largest single count over 14).  At thr = 15 about half of a warp's blocks
 // hold a flagged sweep, and counting it leaves the other lanes idle: single
-// counts there made C2 0.9 % faster.
+// counts there made a batch of 10,000 sets with k from 6 to 14 0.9 % faster.
 constexpr int kIsPairThr = 16;
 // Smallest thr at which single counts are flagged and counted after the block
 // rather than on the spot.  A single count tops 10 in about 0.1 % of the
 // codewords, so few blocks hold a flag; below that, stepping back through
-// digit 1's moves to a flagged sweep costs more than a branch per sweep.  On
-// the mixed-k batch the straight-line blocks made the step 0.3 % faster (the
-// 14-row codes, at thr 14 and 15 on level 4, 4.5 %; the 12-row codes, at
-// thr 11 to 13, 1.2 % slower); starting them at 13 or 14 instead was slower
-// for all three.
+// digit 1's moves to a flagged sweep costs more than a branch per sweep.  The
+// straight-line blocks made a batch of 10,000 sets with k from 6 to 14 0.3 %
+// faster, 1,000 sets of 14 rows (level 4 at thr 14 and 15) 4.5 % faster and
+// 1,000 sets of 12 rows (thr 11 to 13) 1.2 % slower; starting them at thr 13
+// or 14 instead was slower on all three batches.
 constexpr int kIsDeferThr = 10;
 
 // Walks blocks [b0, b0 + nblk) of one support; P is the sum of its rows other
