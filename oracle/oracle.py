@@ -13,7 +13,7 @@ from __future__ import annotations
 import ctypes
 import os
 import subprocess
-from ctypes import POINTER, c_int, c_int32, c_int64, c_uint64, c_void_p
+from ctypes import c_int, c_int64, c_uint64, c_void_p
 from pathlib import Path
 
 import numpy as np
