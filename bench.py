@@ -99,10 +99,6 @@ def make_workload(rank: int, n: int = N_SETS, k_lo: int = K_LO, k_hi: int = K_HI
     return [sorted(rng.choice(49, int(k), replace=False).tolist()) for k in ks]
 
 
-def reference_messages(sets) -> float:
-    return float(sum((8 ** len(s)) - 1 for s in sets))
-
-
 def shard_bounds(n: int, rank: int, world: int) -> tuple[int, int]:
     """Contiguous near-equal shard [lo, hi) of n items for `rank` (used when a
     fixed batch is split across ranks)."""

@@ -97,13 +97,6 @@ def choose(table: dict[int, dict], k_max: int) -> LaunchConfig | None:
     return LaunchConfig(**{key: int(e[key]) for key in _SHAPE_KEYS if key in e})
 
 
-def config_for(device_id: int, k_max: int, path: Path | None = None) -> LaunchConfig | None:
-    from . import _lib
-
-    name = _lib.device_info(device_id)[3]
-    return choose(load_table(name, path), k_max)
-
-
 def calibration_sets(k: int, target_codewords: float = 2e10, seed: int = 97) -> list[list[int]]:
     """Seeded sets of size k whose orbit enumeration is ~target_codewords."""
     per_code = max(1.0, 0.2 * 8.0 ** max(k - 2, 1))
