@@ -557,12 +557,6 @@ __global__ void __launch_bounds__(kScanThreads) scan_level_kernel(DistArgs a, in
   }
 }
 
-__device__ __forceinline__ void is_weight(const V6& p, int& wmin) {
-  const int lo = __popc(lop3<0xFE>(p.l0, p.l1, p.l2));
-  const int hi = __popc(lop3<0xFE>(p.h0, p.h1, p.h2));
-  wmin = __viaddmin_s32(lo, hi, wmin);
-}
-
 // p <- alpha^e p on the bit-sliced planes, e in 0..6.
 __device__ __forceinline__ void v6_alpha_pow(V6& p, int e) {
   for (int i = 0; i < e; ++i) {
@@ -617,11 +611,6 @@ struct WitOut {
   uint8_t* dst;
   int32_t* lock;
 };
-
-__device__ __forceinline__ WitOut wit_out(const DistArgs& a, int c, int j) {
-  return WitOut{a.is_piv + size_t(c) * kIsMaxSets + j, a.witness + size_t(c) * kN,
-                a.wit_lock + c};
-}
 
 // Records a codeword, given in its information set's column order (positions
 // 0..31 in the lo words, 32..48 in bits 0..16 of the hi words), as the code's

@@ -81,7 +81,6 @@ __device__ uint64_t canon_mask_warp(int lane, uint64_t S, const uint8_t* gl2) {
   return canon_mask_warp_min<true>(lane, S, gl2);
 }
 
-__device__ __forceinline__ int srv_stage(int w, int part) { return 2 * w + part - 1; }
 __device__ __forceinline__ int srv_stage_level(int st) { return st >> 1; }
 __device__ __forceinline__ int srv_stage_part(int st) { return (st & 1) + 1; }
 
