@@ -7,6 +7,8 @@ hand-written sm_100a CUDA library:
   DistanceOracleCUDABP, init_cuda_oracles_bp   -- max_zeros / min distance
   CanonicalOracle, init_canon_oracle           -- AGL2(F7) canonical forms
   CanonicalDedup                               -- device hash-set dedup
+  DistanceOracle, init_device, init_devices_all -- the same oracle with the
+      signatures of the reference's OpenCL-era kernel.py / precompute.py
 
 and the drivers built on them: ToricServer (device-resident request loop),
 ToricServerPool (one loop per GPU), ToricBatchServer (micro-batches of the
@@ -19,6 +21,7 @@ from .tables import (  # noqa: F401
     N_POINTS,
     bounding_cube_points,
     build_eval_matrix,
+    eval_monomial,
     gf8_mul,
     gf8_pow,
     indices_of,
@@ -36,12 +39,16 @@ __all__ = [
     "CanonicalOracle",
     "init_canon_oracle",
     "CanonicalDedup",
+    "DistanceOracle",
+    "init_device",
+    "init_devices_all",
     "LaunchConfig",
     "ToricServer",
     "ToricServerPool",
     "ToricBatchServer",
     "CanonicalBFS",
     "build_eval_matrix",
+    "eval_monomial",
     "precompute_gl2_perms",
     "rel_table",
     "unpack_canonical",
@@ -64,6 +71,10 @@ def __getattr__(name):
         from . import serve
 
         return getattr(serve, name)
+    if name in ("DistanceOracle", "init_device", "init_devices_all"):
+        from . import devices
+
+        return getattr(devices, name)
     if name == "CanonicalBFS":
         from . import search
 

@@ -47,12 +47,17 @@ def bounding_cube_points() -> list[tuple[int, int]]:
     return [(i // 7, i % 7) for i in range(N_POINTS)]
 
 
+def eval_monomial(a: tuple[int, int], p: tuple[int, int]) -> int:
+    """x^a0 y^a1 at the torus point p = (x, y) (precompute.py:27-29)."""
+    return gf8_mul(gf8_pow(p[0], a[0]), gf8_pow(p[1], a[1]))
+
+
 def build_eval_matrix() -> np.ndarray:
     """49 x 49 int32 matrix: row a*7+b is x^a y^b at the torus points."""
     m = np.zeros((N_POINTS, N_POINTS), dtype=np.int32)
-    for i, (a, b) in enumerate(bounding_cube_points()):
-        for j, (x, y) in enumerate(torus_points()):
-            m[i, j] = gf8_mul(gf8_pow(x, a), gf8_pow(y, b))
+    for i, a in enumerate(bounding_cube_points()):
+        for j, p in enumerate(torus_points()):
+            m[i, j] = eval_monomial(a, p)
     return m
 
 
