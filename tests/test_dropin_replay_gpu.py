@@ -105,6 +105,55 @@ def test_replay_every_recorded_call(traces, dropin, M):
     assert n_calls > 30
 
 
+@pytest.fixture(scope="module")
+def opencl_dropin():
+    """The drop-in precompute and kernel modules, imported by the reference's
+    names (the OpenCL-era drivers' imports)."""
+    from generalized_toric_gpu_search_b200 import build as lib_build
+
+    lib_build.build()
+    saved = {m: sys.modules.pop(m, None) for m in ("precompute", "kernel")}
+    sys.path.insert(0, str(DROPIN))
+    try:
+        pre = importlib.import_module("precompute")
+        ker = importlib.import_module("kernel")
+        assert Path(pre.__file__).parent == DROPIN and Path(ker.__file__).parent == DROPIN
+        yield pre, ker
+    finally:
+        sys.path.remove(str(DROPIN))
+        for m, v in saved.items():
+            sys.modules.pop(m, None)
+            if v is not None:
+                sys.modules[m] = v
+
+
+def test_replay_through_the_opencl_era_names(traces, opencl_dropin):
+    """The recorded max_zeros_batch calls through DistanceOracle(ctx, queue,
+    M_buf) built from init_opencl(), as champion_search.py:265-266 builds it,
+    and single-set max_zeros on the first sets of each exact call."""
+    pre, ker = opencl_dropin
+    ctx, queue, M_buf, M = pre.init_opencl()
+    assert np.array_equal(M, pre.build_eval_matrix())
+    o = ker.DistanceOracle(ctx, queue, M_buf)
+    n_calls = 0
+    for name, sc in traces["scenarios"].items():
+        for c in sc["calls"]:
+            if c["api"] != "max_zeros_batch" or c["device_id"] != 0:
+                continue
+            n_calls += 1
+            batch = rows(c["sets"])
+            td = c["target_distance"]
+            got = o.max_zeros_batch(batch, td, c["sample_count"], c["sample_seed"])
+            if td <= 1:
+                assert got == c["result"], name
+            else:
+                _check_max_zeros(got, c["result"], td)
+            if c["sample_count"] == 0:
+                single = [o.max_zeros(s, td) for s in batch[:4]]
+                _check_max_zeros(single, c["result"][:4], max(td, 1))
+    assert n_calls > 10
+
+
 def _by_kind(records):
     out: dict = {}
     for r in records:
