@@ -947,7 +947,10 @@ __device__ __forceinline__ unsigned long long is_walk_blocks(
   // The move into block m = b0 + i + 1 changes digit 2 when m % 7 != 0 (six
   // blocks in seven): up from alpha^(m7 - 1) when m / 7 is even, else down
   // from alpha^(7 - m7); the rest take the general form.
-  const int n = int(nblk);  // at most 343
+  // A task's blocks in one support: at most 343 in the batch walk; the served
+  // loop's largest stages (k >= 15) take 343 x 7^j so their task count fits
+  // the claim word.
+  const int n = int(nblk);
   int m7 = int((b0 + 1ull) % 7ull);
   int par = int(((b0 + 1ull) / 7ull) & 1ull);
   V6 nx;
