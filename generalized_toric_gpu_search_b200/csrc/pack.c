@@ -15,8 +15,8 @@
  *       staging buffers that the host-to-device copy reads directly) at the
  *       given addresses, of flat_cap int32 and off_cap int64 elements.  When
  *       the batch needs more (total > flat_cap or len(batch) + 1 > off_cap) it
- *       writes nothing and returns done = False with the sizes in total and
- *       k_max.
+ *       returns done = False with the sizes in total and k_max; the arrays'
+ *       contents are then unspecified (a first pass may have started them).
  *
  * batch is a sequence of sequences of ints.  `bad` is True when an index lies
  * outside 0..48; such values are stored as given when they fit int32 and as -1
@@ -100,6 +100,70 @@ static int fill_batch(const Batch* b, int32_t* f, int64_t* o, int* bad) {
   return 0;
 }
 
+/* One pass over a list or tuple of lists or tuples of exact ints that fit a
+ * machine word (what the drivers pass), straight into the caller's arrays: no
+ * size pass, no references taken, and the next sets' objects prefetched (the
+ * loop is bound by the latency of reaching each set's items).  No Python code
+ * runs inside it, so nothing can change the batch under it.  Returns 1 when
+ * the batch is written, 0 when it does not fit the capacities or holds
+ * anything else (the caller then takes the general path, which also reports
+ * the sizes). */
+static int fill_direct(PyObject* batch, int32_t* f, Py_ssize_t fcap, int64_t* o,
+                       Py_ssize_t ocap, Py_ssize_t* total, Py_ssize_t* k_max, int* bad) {
+#if PY_VERSION_HEX >= 0x030C0000
+  PyObject** sets;
+  Py_ssize_t n;
+  if (PyList_CheckExact(batch)) {
+    sets = ((PyListObject*)batch)->ob_item;
+    n = PyList_GET_SIZE(batch);
+  } else if (PyTuple_CheckExact(batch)) {
+    sets = ((PyTupleObject*)batch)->ob_item;
+    n = PyTuple_GET_SIZE(batch);
+  } else {
+    return 0;
+  }
+  if (n + 1 > ocap) return 0;
+  Py_ssize_t pos = 0, km = 0;
+  int any_bad = 0;
+  o[0] = 0;
+  for (Py_ssize_t i = 0; i < n; ++i) {
+    if (i + 8 < n) __builtin_prefetch(sets[i + 8]);
+    if (i + 4 < n && PyList_CheckExact(sets[i + 4]))
+      __builtin_prefetch(((PyListObject*)sets[i + 4])->ob_item);
+    PyObject* s = sets[i];
+    PyObject** items;
+    Py_ssize_t k;
+    if (PyList_CheckExact(s)) {
+      items = ((PyListObject*)s)->ob_item;
+      k = PyList_GET_SIZE(s);
+    } else if (PyTuple_CheckExact(s)) {
+      items = ((PyTupleObject*)s)->ob_item;
+      k = PyTuple_GET_SIZE(s);
+    } else {
+      return 0;
+    }
+    if (pos + k > fcap) return 0;
+    for (Py_ssize_t j = 0; j < k; ++j) {
+      PyObject* it = items[j];
+      if (!PyLong_CheckExact(it) || !PyUnstable_Long_IsCompact((PyLongObject*)it)) return 0;
+      const long v = (long)PyUnstable_Long_CompactValue((PyLongObject*)it);
+      any_bad |= (unsigned long)v > 48ul;
+      f[pos + j] = (v < INT32_MIN || v > INT32_MAX) ? -1 : (int32_t)v;
+    }
+    pos += k;
+    if (k > km) km = k;
+    o[i + 1] = (int64_t)pos;
+  }
+  *total = pos;
+  *k_max = km;
+  *bad = any_bad;
+  return 1;
+#else
+  (void)batch, (void)f, (void)fcap, (void)o, (void)ocap, (void)total, (void)k_max, (void)bad;
+  return 0;
+#endif
+}
+
 static PyObject* pack(PyObject* self, PyObject* args) {
   PyObject* batch;
   (void)self;
@@ -133,6 +197,13 @@ static PyObject* pack_into(PyObject* self, PyObject* args) {
   (void)self;
   if (!PyArg_ParseTuple(args, "OKnKn", &batch, &flat_addr, &flat_cap, &off_addr, &off_cap))
     return NULL;
+  {
+    Py_ssize_t total = 0, k_max = 0;
+    int bad = 0;
+    if (fill_direct(batch, (int32_t*)(uintptr_t)flat_addr, flat_cap, (int64_t*)(uintptr_t)off_addr,
+                    off_cap, &total, &k_max, &bad))
+      return Py_BuildValue("(nnOO)", total, k_max, bad ? Py_True : Py_False, Py_True);
+  }
   Batch b;
   PyObject* result = NULL;
   if (collect_batch(batch, &b) == 0) {

@@ -85,12 +85,14 @@ def test_pack_into_caller_buffers(packer):
     total = int(off_ref[-1])
     f = np.full(total + 5, -7, np.int32)
     o = np.zeros(len(batch) + 1, np.int64)
-    # too small: nothing written, sizes reported
+    # too small: sizes reported, nothing written past the given capacities
     assert packer.pack_into(batch, f.ctypes.data, total - 1, o.ctypes.data, o.size) == (
         total, k_max, False, False)
-    assert (f == -7).all() and not o.any()
+    assert (f[total - 1:] == -7).all()
+    o[:] = 0
     assert packer.pack_into(batch, f.ctypes.data, f.size, o.ctypes.data, len(batch)) == (
         total, k_max, False, False)
+    assert not o.any()
     # enough room: the same arrays as pack()
     assert packer.pack_into(batch, f.ctypes.data, f.size, o.ctypes.data, o.size) == (
         total, k_max, bad, True)
@@ -101,6 +103,30 @@ def test_pack_into_caller_buffers(packer):
     assert packer.pack_into([[1, 50]], f.ctypes.data, f.size, o.ctypes.data, o.size)[2]
     with pytest.raises(TypeError):
         packer.pack_into([[1, "a"]], f.ctypes.data, f.size, o.ctypes.data, o.size)
+
+
+@pytest.mark.parametrize("batch", [
+    [[3, 4], (5, 6, 7)],                        # lists and tuples: the one-pass path
+    ((3, 4), [5, 6, 7]),                        # a tuple batch
+    [[3, 4], np.array([5, 6, 7])],              # an array set: the general path
+    [[3, np.int64(4)], [5, 6, 7]],              # a numpy int in a list
+    [[3, True], [5, 6, 7]],                     # a bool (an int subclass)
+    [[3, 2**40], [5, -1, 7]],                   # a multi-digit int and a negative one
+    [[3, 4], [5, 6, 7]] * 1000,                 # long enough to reach the prefetches
+])
+def test_pack_into_paths_agree_with_pack(packer, batch):
+    """The one-pass path (lists or tuples of exact small ints) and the
+    general path write what pack() returns, whichever the batch takes."""
+    flat_b, off_b, k_max, bad = packer.pack(batch)
+    off_ref = np.frombuffer(off_b, np.int64)
+    total = int(off_ref[-1])
+    f = np.full(total + 3, -7, np.int32)
+    o = np.zeros(len(batch) + 1, np.int64)
+    assert packer.pack_into(batch, f.ctypes.data, f.size, o.ctypes.data, o.size) == (
+        total, k_max, bad, True)
+    np.testing.assert_array_equal(f[:total], np.frombuffer(flat_b, np.int32)[:total])
+    np.testing.assert_array_equal(o, off_ref)
+    assert (f[total:] == -7).all()
 
 
 @pytest.fixture
