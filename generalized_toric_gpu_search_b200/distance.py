@@ -452,7 +452,7 @@ class DistanceOracleCUDABP:
             status = runner.status(p, s)  # synchronises the stream
         if status != _lib.TG_OK:
             _lib.check(status, "max_zeros_batch_witness (device)")
-        return h_out.tolist(), h_wit.numpy()
+        return h_out.numpy().tolist(), h_wit.numpy()
 
     def min_distance(self, s_indices: list[int], target_distance: int = 1) -> int:
         """49 - max_zeros (the helper of kernel backup.py:161-163)."""
@@ -503,7 +503,7 @@ class DistanceOracleCUDABP:
             status = self.runner.status(p, s)  # synchronises the stream
         if status != _lib.TG_OK:
             _lib.check(status, "max_zeros_batch (device)")
-        return h_out.tolist()
+        return h_out.numpy().tolist()  # numpy converts faster than torch
 
 
 def init_cuda_oracles_bp(M: np.ndarray) -> tuple[list[DistanceOracleCUDABP], int]:
