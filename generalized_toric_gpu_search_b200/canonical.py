@@ -106,14 +106,7 @@ class CanonicalOracle:
         if n == 0:
             return np.zeros(0, dtype=object)
         _, lo, hi = self._run_sets(arr)
-        # Python ints lo + hi * 2**64, as the reference returns them; the high
-        # word is zero up to k = 11, so only the rows that have one pay for it
-        # (half the host time of a million k <= 10 keys).
-        out = lo.astype(object)
-        nz = np.flatnonzero(hi)
-        if nz.size:
-            out[nz] = out[nz] + (hi[nz].astype(object) << 64)
-        return out
+        return keys_from_words(lo, hi)
 
     def compute_masks(self, sets) -> np.ndarray:
         """Rows of any size 1..49 (or an (n,) array of 49-bit masks as uint64)
@@ -151,6 +144,19 @@ def _pick_rel_table(rel_table, rel_table_arr):
     if rel_table is not None and rel_table_arr is not None:
         raise TypeError("pass rel_table or rel_table_arr, not both")
     return rel_table if rel_table is not None else rel_table_arr
+
+
+def keys_from_words(lo: np.ndarray, hi: np.ndarray) -> np.ndarray:
+    """(n,) object array of the Python ints lo + hi * 2**64, the form of the
+    reference's keys (kernel_canon.py:174-176).  The high word is zero up to
+    k = 11, so only the rows that have one pay for the wide arithmetic (half
+    the host time of a million k <= 10 keys)."""
+    out = np.asarray(lo, dtype=np.uint64).astype(object)
+    hi = np.asarray(hi, dtype=np.uint64)
+    nz = np.flatnonzero(hi)
+    if nz.size:
+        out[nz] = out[nz] + (hi[nz].astype(object) << 64)
+    return out
 
 
 def init_canon_oracle(device_id: int, gl2_perms: np.ndarray | None = None,

@@ -9,7 +9,8 @@ top row its anchored translates can reach, depends on A's first row alone;
 the table lists the matrices by (a, b, c, d), 42 per first row.  The kernel
 keeps only the first rows that reach the overall smallest top row.  This test
 checks, on random sets of every size, that the minimum over those first rows
-equals the minimum over all 2016 matrices.
+equals the minimum over all 2016 matrices.  The last test checks the host
+assembly of compute()'s packed keys.
 """
 
 from __future__ import annotations
@@ -58,3 +59,19 @@ def test_first_row_prefilter_keeps_the_minimum(size):
         kept = [g * 42 + j for g in range(48) if tops[g] == tstar for j in range(42)]
         assert canonical_brute(S, kept) == canonical_brute(S, range(2016))
         assert (canonical_brute(S, kept).bit_length() - 1) // 7 == tstar
+
+
+def test_keys_from_words_matches_the_reference_formula():
+    """compute()'s key assembly: Python ints lo + hi * 2**64
+    (kernel_canon.py:174-176), whether or not a row has a high word."""
+    from generalized_toric_gpu_search_b200.canonical import keys_from_words
+
+    rng = np.random.default_rng(3)
+    lo = rng.integers(0, 2**63, 5000, dtype=np.uint64) * np.uint64(2) + np.uint64(1)
+    for hi in (np.zeros(5000, np.uint64), rng.integers(0, 2**32, 5000, dtype=np.uint64),
+               np.where(rng.random(5000) < 0.1, np.uint64(7), np.uint64(0))):
+        got = keys_from_words(lo, hi)
+        want = lo.astype(object) + hi.astype(object) * (1 << 64)
+        assert got.dtype == object and len(got) == 5000
+        assert all(type(g) is int and g == w for g, w in zip(got, want))
+    assert len(keys_from_words(np.zeros(0, np.uint64), np.zeros(0, np.uint64))) == 0
