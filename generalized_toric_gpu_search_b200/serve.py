@@ -535,7 +535,7 @@ class ToricBatchServer:
         _, cw, _ = runner.counters(s)
         with self._cv:
             self._stats["codewords"] += cw
-        return h_out.tolist(), e0.elapsed_time(e1) / 1e3
+        return h_out.numpy().tolist(), e0.elapsed_time(e1) / 1e3
 
     def _serve(self, batch) -> None:
         n = len(batch)
